@@ -1,0 +1,667 @@
+"""Generate the golden fixtures in this folder.
+
+An independent pure-Python transcription of TrackPad.jl's per-particle maps
+(src/tracking.jl) and of linepass!/ringpass! (src/lattice.jl:260-317), written
+separately from the C++ oracle so that the two transcriptions check each other.
+Python floats are IEEE binary64 with no fused multiply-add and `math` calls the
+C library, so the oracle must reproduce these numbers bit for bit.
+
+The cases are the reference's own parity tests, run on its own 10-particle
+fixture (test/verify_elements.jl:10-21, energy 3.5e9 eV):
+  * every element case of test/verify_elements.jl:48-118 this engine supports,
+  * the FODO line of test/verify_fodo.jl:30-39,
+  * the DBA line of test/verify_dba.jl:31-44,
+  * the single bends of test/verify_bend.jl:25-28 and
+    test/verify_exact_bend.jl:24-28,
+plus multi-turn and loss cases on the same fixture.
+
+Usage:  python tests/golden/make_golden.py   (writes golden_*.json here)
+"""
+import json
+import math
+import os
+
+NAN = float("nan")
+COORD_LIMIT = 1.0  # tracking.jl:25
+ANGLE_LIMIT = 1.0  # tracking.jl:26
+DRIFT1 = 0.6756035959798286638  # tracking.jl:29-32
+DRIFT2 = -0.1756035959798286639
+KICK1 = 1.351207191959657328
+KICK2 = -1.702414383919314656
+C_LIGHT = 2.99792458e8  # elements/rf.jl:28
+M_ELECTRON = 0.51099895069e6  # lattice.jl:42
+TWO_PI = 2.0 * math.pi
+EPS = 2.220446049250313e-16
+
+PARTICLES = [  # test/verify_elements.jl:10-21 (rows = particles)
+    [1.0e-4, 2.0e-4, 3.0e-4, -1.0e-4, 5.0e-5, 2.0e-4],
+    [-2.2e-4, 1.7e-4, -1.1e-4, 2.3e-4, -7.0e-5, 1.0e-4],
+    [3.5e-4, -2.1e-4, 8.0e-5, -1.8e-4, 1.4e-4, -2.6e-4],
+    [-4.0e-4, 2.9e-4, 1.6e-4, 9.0e-5, -1.2e-4, 3.1e-4],
+    [5.2e-4, -3.3e-4, -2.4e-4, 1.1e-4, 2.6e-4, -3.7e-4],
+    [-6.1e-4, 4.4e-4, 2.7e-4, -2.5e-4, -3.0e-4, 4.5e-4],
+    [7.0e-4, -5.2e-4, -3.1e-4, 3.4e-4, 3.3e-4, -5.0e-4],
+    [-8.0e-4, 6.0e-4, 3.9e-4, -4.2e-4, -3.8e-4, 5.8e-4],
+    [9.1e-4, -6.7e-4, -4.6e-4, 5.1e-4, 4.4e-4, -6.3e-4],
+    [-9.8e-4, 7.3e-4, 5.3e-4, -5.9e-4, -4.9e-4, 7.1e-4],
+]
+
+
+def beti_of(energy, mass=M_ELECTRON):
+    """Beam(energy): gamma=(E+m)/m, beta=sqrt(1-1/gamma^2); beti=1/beta (lattice.jl:50-61)."""
+    gamma = (energy + mass) / mass
+    beta = math.sqrt(1.0 - 1.0 / (gamma * gamma))
+    return 1.0 / beta
+
+
+def nan6():
+    return (NAN,) * 6
+
+
+# --------------------------------------------------------------------------
+# Element constructors with the reference defaults (src/elements/*.jl)
+# --------------------------------------------------------------------------
+def elem(kind, **kw):
+    e = dict(kind=kind, max_order=0, num_int_steps=0, fringe_bend_entrance=0, fringe_bend_exit=0,
+             misalign_index=-1, iparam=[0, 0], L=0.0, k=0.0, angle=0.0, e1=0.0, e2=0.0, fint1=0.0,
+             fint2=0.0, gap=0.0, gk=0.0, polynom_a=[0.0] * 4, polynom_b=[0.0] * 4, kick_angle=[0.0, 0.0],
+             volt=0.0, freq=0.0, h=0.0, lag=0.0, philag=0.0, energy=0.0, param=[0.0] * 8)
+    e.update(kw)
+    return e
+
+
+def Marker():
+    return elem("MARKER")
+
+
+def Drift(L):
+    return elem("DRIFT", L=float(L))
+
+
+def Quadrupole(L, k1, num_int_steps=10, max_order=1):  # elements/quad.jl:26-47
+    return elem("QUADRUPOLE", L=float(L), k=float(k1), num_int_steps=num_int_steps, max_order=max_order)
+
+
+def Sextupole(L, k2, num_int_steps=10, max_order=2):  # elements/multipole.jl:26-47
+    return elem("SEXTUPOLE", L=float(L), k=float(k2), num_int_steps=num_int_steps, max_order=max_order)
+
+
+def Octupole(L, k3, num_int_steps=10, max_order=3):  # elements/multipole.jl:72-93
+    return elem("OCTUPOLE", L=float(L), k=float(k3), num_int_steps=num_int_steps, max_order=max_order)
+
+
+def ThinMultipole(L, pa, pb, max_order=1):  # elements/multipole.jl:118-139
+    return elem("THIN_MULTIPOLE", L=float(L), polynom_a=[float(v) for v in pa],
+                polynom_b=[float(v) for v in pb], max_order=max_order, num_int_steps=1)
+
+
+def SBend(L, angle, e1=0.0, e2=0.0, num_int_steps=10, fbe=1, fbx=1, fint1=0.0, fint2=0.0, gap=0.0):
+    return elem("SBEND", L=float(L), angle=float(angle), e1=float(e1), e2=float(e2), num_int_steps=num_int_steps,
+                fringe_bend_entrance=fbe, fringe_bend_exit=fbx, fint1=fint1, fint2=fint2, gap=gap)
+
+
+def RBend(L, angle, **kw):  # elements/bend.jl:81
+    return SBend(L, angle, angle / 2, angle / 2, **kw)
+
+
+def ExactSBend(L, angle, e1=0.0, e2=0.0, num_int_steps=10, gk=0.0, fbe=1, fbx=1):
+    return elem("EXACT_SBEND", L=float(L), angle=float(angle), e1=float(e1), e2=float(e2),
+                num_int_steps=num_int_steps, gk=float(gk), fringe_bend_entrance=fbe, fringe_bend_exit=fbx)
+
+
+def ERBend(L, angle, **kw):  # elements/SCelements.jl:339
+    return ExactSBend(L, angle, angle / 2, angle / 2, **kw)
+
+
+def RFCavity(L, volt, freq, lag=0.0, h=1.0, philag=0.0, energy=0.0):  # elements/rf.jl:16-21
+    return elem("RFCAVITY", L=float(L), volt=float(volt), freq=float(freq), lag=float(lag), h=float(h),
+                philag=float(philag), energy=float(energy))
+
+
+def Solenoid(L, ks):
+    return elem("SOLENOID", L=float(L), param=[float(ks)] + [0.0] * 7)
+
+
+def Corrector(L, hk, vk):
+    return elem("CORRECTOR", L=float(L), param=[float(hk), float(vk)] + [0.0] * 6)
+
+
+def Translation(L, dx=0.0, dy=0.0, ds=0.0):
+    return elem("TRANSLATION", L=float(L), param=[dx, dy, ds] + [0.0] * 5)
+
+
+def YRotation(L, angle=0.0):
+    return elem("YROTATION", L=float(L), angle=float(angle))
+
+
+def CrabCavity(L, volt=0.0, freq=0.0, phi=0.0, energy=1.0e9):  # elements/rf.jl:46-53
+    k = TWO_PI * freq / C_LIGHT
+    return elem("CRAB_CAVITY", L=float(L), volt=volt, freq=freq, energy=energy,
+                param=[k, phi, 0.0, 0.0] + [0.0] * 4)
+
+
+def AccelCavity(L, volt=0.0, freq=0.0, h=1.0, phis=0.0, energy=1.0e9):  # elements/rf.jl:80-87
+    k = TWO_PI * freq / C_LIGHT
+    return elem("ACCEL_CAVITY", L=float(L), volt=volt, freq=freq, h=h, energy=energy,
+                param=[k, phis] + [0.0] * 6)
+
+
+def LongitudinalRFMap(alphac, rf):  # _rf_k/_rf_h: tracking.jl:1565-1573
+    if rf["kind"] == "RFCAVITY":
+        k, h = TWO_PI * rf["freq"] / C_LIGHT, rf["h"]
+    elif rf["kind"] == "ACCEL_CAVITY":
+        k, h = rf["param"][0], rf["h"]
+    elif rf["kind"] == "CRAB_CAVITY":
+        k, h = rf["param"][0], 1.0
+    else:
+        k, h = 0.0, 1.0
+    return elem("LONGITUDINAL_RF_MAP", param=[alphac, k, h] + [0.0] * 5)
+
+
+def LorentzBoost(angle, mode=0):  # elements/beambeam.jl:14-19
+    return elem("LORENTZ_BOOST", param=[angle, math.cos(angle), 0.0, math.tan(angle)] + [0.0] * 4, iparam=[mode, 0])
+
+
+def InvLorentzBoost(angle, mode=0):  # elements/beambeam.jl:38-43
+    return elem("INV_LORENTZ_BOOST", param=[angle, math.cos(angle), math.sin(angle), 0.0] + [0.0] * 4,
+                iparam=[mode, 0])
+
+
+def DriftSC(L):
+    return elem("DRIFT_SC", L=float(L))
+
+
+def QuadrupoleSC(L, k0=0.0, k1=0.0, k2=0.0, k3=0.0, max_order=1, num_int_steps=10):
+    return elem("QUADRUPOLE_SC", L=float(L), param=[k0, k1, k2, k3] + [0.0] * 4, max_order=max_order,
+                num_int_steps=num_int_steps)
+
+
+def SextupoleSC(L, k0=0.0, k1=0.0, k2=0.0, k3=0.0, max_order=2, num_int_steps=10):
+    return elem("SEXTUPOLE_SC", L=float(L), param=[k0, k1, k2, k3] + [0.0] * 4, max_order=max_order,
+                num_int_steps=num_int_steps)
+
+
+def OctupoleSC(L, k0=0.0, k1=0.0, k2=0.0, k3=0.0, max_order=3, num_int_steps=10):
+    return elem("OCTUPOLE_SC", L=float(L), param=[k0, k1, k2, k3] + [0.0] * 4, max_order=max_order,
+                num_int_steps=num_int_steps)
+
+
+def SBendSC(L, angle, e1=0.0, e2=0.0, num_int_steps=10):
+    return elem("SBEND_SC", L=float(L), angle=float(angle), e1=float(e1), e2=float(e2),
+                num_int_steps=num_int_steps, fringe_bend_entrance=1, fringe_bend_exit=1)
+
+
+def SpaceCharge(L):
+    return elem("SPACE_CHARGE", L=float(L))
+
+
+def StrongThinGaussianBeam(amplitude, rmssizex, rmssizey, xoffset=0.0, yoffset=0.0):
+    return elem("STRONG_THIN_GAUSSIAN_BEAM", param=[amplitude, rmssizex, rmssizey, xoffset, yoffset, 0.0, 0.0, 0.0])
+
+
+# --------------------------------------------------------------------------
+# Maps (src/tracking.jl), written over 6-tuples
+# --------------------------------------------------------------------------
+def lost_check(r):  # tracking.jl:49-52
+    return (math.isnan(r[0]) or abs(r[0]) > COORD_LIMIT or abs(r[2]) > COORD_LIMIT
+            or abs(r[1]) > ANGLE_LIMIT or abs(r[3]) > ANGLE_LIMIT)
+
+
+def drift(r, L, beti):  # tracking.jl:87-99 (exact Hamiltonian branch)
+    x, px, y, py, z, d = r
+    pz2 = 1.0 + 2.0 * d * beti + d * d - px * px - py * py
+    if pz2 <= 0.0:
+        return nan6()
+    nl = L / math.sqrt(pz2)
+    return (x + nl * px, px, y + nl * py, py, z + nl * (beti + d) - L * beti, d)
+
+
+def horner(pa, pb, order, x, y):  # shared Horner loop of tracking.jl:243-305
+    re, im = pb[order], pa[order]
+    for i in range(order - 1, -1, -1):
+        re, im = re * x - im * y + pb[i], im * x + re * y + pa[i]
+    return re, im
+
+
+def thin_kick(r, pa, pb, K, order):  # strthinkick, tracking.jl:284-305
+    re, im = horner(pa, pb, order, r[0], r[2])
+    return (r[0], r[1] - K * re, r[2], r[3] + K * im, r[4], r[5])
+
+
+def bend_kick(r, pa, pb, K, irho, order, beti):  # bndthinkick, tracking.jl:243-270
+    re, im = horner(pa, pb, order, r[0], r[2])
+    return (r[0], r[1] - K * (re - (r[5] - r[0] * irho) * irho), r[2], r[3] + K * im,
+            r[4] + K * irho * r[0] * beti, r[5])
+
+
+def yoshida(r, L, steps, drift_fn, kick_fn):  # tracking.jl:317-375
+    sl = L / float(steps)
+    l1, l2, k1, k2 = sl * DRIFT1, sl * DRIFT2, sl * KICK1, sl * KICK2
+    for _ in range(steps):
+        r = drift_fn(r, l1)
+        r = kick_fn(r, k1)
+        r = drift_fn(r, l2)
+        r = kick_fn(r, k2)
+        r = drift_fn(r, l2)
+        r = kick_fn(r, k1)
+        r = drift_fn(r, l1)
+    return r
+
+
+def folded(e, pa, pb):  # kick_angle folding, tracking.jl:396-411
+    pa, pb = list(pa), list(pb)
+    if e["L"] > 0.0:
+        pb[0] = pb[0] - math.sin(e["kick_angle"][0]) / e["L"]
+        pa[0] = pa[0] + math.sin(e["kick_angle"][1]) / e["L"]
+    return pa, pb
+
+
+def edge(r, irho, ang, fint, gap, method, at_exit):  # tracking.jl:160-221
+    if fint == 0.0 or gap == 0.0 or method == 0:
+        fc = 0.0
+    else:
+        se, ce = math.sin(ang), math.cos(ang)
+        fc = irho * gap * fint * (1.0 + se * se) / ce
+    fx = irho * math.tan(ang)
+    opd = 1.0 + r[5]
+    if method == 2:
+        fy = irho * math.tan(ang - fc / opd) / opd
+    elif method == 3:
+        fy = irho * math.tan(ang - fc - r[1] / opd) if at_exit else irho * math.tan(ang - fc + r[1] / opd)
+    else:
+        fy = irho * math.tan(ang - fc / opd)
+    return (r[0], r[1] + r[0] * fx, r[2], r[3] - r[2] * fy, r[4], r[5])
+
+
+def pxyz(dp1, px, py):  # tracking.jl:717-720
+    v = dp1 * dp1 - px * px - py * py
+    return math.sqrt(v) if v > 0.0 else 0.0
+
+
+def jclamp(v):  # Julia clamp(v, -1, 1); NaN passes through
+    return 1.0 if v > 1.0 else (-1.0 if v < -1.0 else v)
+
+
+def yrot(r, phi, beti):  # tracking.jl:727-745
+    if phi == 0.0:
+        return r
+    x, px, y, py, z, d = r
+    dp1 = beti + d
+    c, s = math.cos(phi), math.sin(phi)
+    pz = pxyz(dp1, px, py)
+    p = c * pz - s * px
+    return (x * pz / p, s * pz + c * px, y + x * py * s / p, py, z + dp1 * x * s / p, d)
+
+
+def fringe(r, irho, gk, beti):  # bend_fringe, tracking.jl:752-815
+    x, px, y, py, z, d = r
+    b0 = irho
+    dp1 = beti + d
+    pz = pxyz(dp1, px, py)
+    xp, yp = px / pz, py / pz
+    t1 = 1.0 + xp * xp * (2.0 + yp * yp)
+    t2 = xp / (1.0 + yp * yp)
+    phi = -b0 * math.tan(b0 * gk * t1 * pz - math.atan(t2))
+    px2, py2, pz2 = px * px, py * py, pz * pz
+    pz4 = pz2 * pz2
+    s2 = py2 + pz2
+    arg = (b0 * gk * (pz4 + px2 * (py2 + 2.0 * pz2))) / (pz2 * pz) - math.atan(px * pz / (py2 + pz2))
+    sec = 1.0 / math.cos(arg)
+    psec = sec * sec
+    py4 = py2 * py2
+    py6 = py4 * py2
+    pz5 = pz4 * pz
+    pz6 = pz4 * pz2
+    s2sq = s2 * s2
+    den = pz5 * (py4 + px2 * pz2 + 2.0 * py2 * pz2 + pz4)
+    dpx = -(b0 * (px2 * pz4 * (py2 - pz2) - pz6 * (py2 + pz2)
+                  + b0 * gk * px * (pz2 * s2sq * (2.0 * py2 + 3.0 * pz2)
+                                    + px2 * px2 * (3.0 * py2 * pz2 + 2.0 * pz4)
+                                    + px2 * (3.0 * py6 + 8.0 * py4 * pz2 + 9.0 * py2 * pz4 + 5.0 * pz6)))) * psec
+    dpx = dpx / den
+    dpy = -(b0 * py * (px * pz4 * (py2 + pz2)
+                       + b0 * gk * (-(pz4 * s2sq) + px2 * px2 * (3.0 * py2 * pz2 + 4.0 * pz4)
+                                    + px2 * (3.0 * py6 + 10.0 * py4 * pz2 + 11.0 * py2 * pz4 + 3.0 * pz6)))) * psec
+    dpy = dpy / den
+    dd = (b0 * dp1 * (px * pz4 * (py2 - pz2)
+                      + b0 * gk * (-(pz4 * s2sq) + px2 * px2 * (3.0 * py2 * pz2 + 2.0 * pz4)
+                                   + px2 * (3.0 * py6 + 8.0 * py4 * pz2 + 7.0 * py2 * pz4 + pz6)))) * psec
+    dd = dd / den
+    yf = (2.0 * y) / (1.0 + math.sqrt(1.0 - 2.0 * dpy * y))
+    return (x + 0.5 * dpx * (yf * yf), px, yf, py - phi * yf, z - 0.5 * dd * (yf * yf), d)
+
+
+def wedge(r, h, theta, beti):  # bend_edge, tracking.jl:822-851
+    if abs(h) < 1e-6:
+        return r
+    x, px, y, py, z, d = r
+    dp1 = beti + d
+    c, s = math.cos(theta), math.sin(theta)
+    pz = pxyz(dp1, px, py)
+    d2 = pxyz(dp1, 0.0, py)
+    pxn = px * c + (pz - h * x) * s
+    das = math.asin(jclamp(px / d2)) - math.asin(jclamp(pxn / d2))
+    num = x * (px * math.sin(2.0 * theta) + s * s * (2.0 * pz - h * x))
+    den = pxyz(dp1, pxn, py) + pz * c - px * s
+    return (x * c + num / den, pxn, y + py * (theta / h + das / h), py, z + dp1 / h * (theta + das), d)
+
+
+def body(r, h, L, beti):  # exact_bend_body, tracking.jl:858-894
+    x, px, y, py, z, d = r
+    dp1 = beti + d
+    pz = pxyz(dp1, px, py)
+    if abs(h) < 1e-6:
+        nl = L / pz
+        return (x + px * nl, px, y + py * nl, py, z + nl * dp1 - L * beti, d)
+    pzmx = pz - (1.0 + x * h)
+    cs, sn = math.cos(h * L), math.sin(h * L)
+    pxn = px * cs + pzmx * sn
+    d2 = pxyz(dp1, 0.0, py)
+    das = L + (math.asin(jclamp(px / d2)) - math.asin(jclamp(pxn / d2))) / h
+    xn = (pxyz(dp1, pxn, py) - pzmx * cs + px * sn - 1.0) / h
+    return (xn, pxn, y + py * das, py, z + dp1 * das - L * beti, d)
+
+
+def apply_pass(e, r, beti):
+    """pass!(elem, r, beti) for every supported element kind."""
+    kind = e["kind"]
+    if kind in ("MARKER", "SPACE_CHARGE"):
+        return r
+    if kind in ("DRIFT", "DRIFT_SC"):
+        return drift(r, e["L"], beti)
+    if kind in ("QUADRUPOLE", "SEXTUPOLE", "OCTUPOLE", "QUADRUPOLE_SC", "SEXTUPOLE_SC", "OCTUPOLE_SC"):
+        pb = list(e["polynom_b"])
+        pa = list(e["polynom_a"])
+        order = e["max_order"]
+        if kind == "QUADRUPOLE":
+            pb[1] = e["k"]
+            pa, pb = folded(e, pa, pb)
+        elif kind == "SEXTUPOLE":
+            pb[2] = e["k"] / 2.0
+        elif kind == "OCTUPOLE":
+            pb[3] = e["k"] / 6.0
+        else:  # SC family: (k0, k1, k2/2, k3/6), tracking.jl:993-1039
+            p = e["param"]
+            pb = [p[0], p[1], p[2] / 2.0, p[3] / 6.0]
+            if kind == "QUADRUPOLE_SC":
+                pa, pb = folded(e, pa, pb)
+            order = min(max(order, 0), 3)
+        return yoshida(r, e["L"], e["num_int_steps"], lambda q, l: drift(q, l, beti),
+                       lambda q, kk: thin_kick(q, pa, pb, kk, order))
+    if kind == "THIN_MULTIPOLE":
+        return thin_kick(r, e["polynom_a"], e["polynom_b"], 1.0, e["max_order"])
+    if kind in ("SBEND", "SBEND_SC"):
+        if kind == "SBEND_SC" and e["L"] == 0.0:
+            return nan6()
+        order = e["max_order"] if kind == "SBEND" else min(max(e["max_order"], 0), 3)
+        irho = e["angle"] / e["L"]
+        pa, pb = folded(e, e["polynom_a"], e["polynom_b"])
+        if e["fringe_bend_entrance"] != 0:
+            r = edge(r, irho, e["e1"], e["fint1"], e["gap"], e["fringe_bend_entrance"], False)
+        r = yoshida(r, e["L"], e["num_int_steps"], lambda q, l: drift(q, l, beti),
+                    lambda q, kk: bend_kick(q, pa, pb, kk, irho, order, beti))
+        if e["fringe_bend_exit"] != 0:
+            r = edge(r, irho, e["e2"], e["fint2"], e["gap"], e["fringe_bend_exit"], True)
+        return r
+    if kind == "EXACT_SBEND":
+        irho = e["angle"] / e["L"]
+        r = yrot(r, e["e1"], beti)
+        if e["fringe_bend_entrance"] != 0:
+            r = fringe(r, irho, e["gk"], beti)
+        r = wedge(r, irho, -e["e1"], beti)
+        if e["num_int_steps"] == 0:
+            r = body(r, irho, e["L"], beti)
+        else:
+            pa, pb = folded(e, e["polynom_a"], e["polynom_b"])
+            r = yoshida(r, e["L"], e["num_int_steps"], lambda q, l: body(q, irho, l, beti),
+                        lambda q, kk: thin_kick(q, pa, pb, kk, e["max_order"]))
+        r = wedge(r, irho, -e["e2"], beti)
+        if e["fringe_bend_exit"] != 0:
+            r = fringe(r, -irho, e["gk"], beti)
+        return yrot(r, e["e2"], beti)
+    if kind == "RFCAVITY":  # tracking.jl:502-518
+        beta = 1.0 / beti
+        if e["L"] > 0.0:
+            r = drift(r, e["L"] / 2.0, beti)
+        if e["energy"] > 0.0:
+            nv = e["volt"] / e["energy"]
+            ph = TWO_PI * e["freq"] * ((r[4] - e["lag"]) / C_LIGHT) - e["philag"]
+            r = r[:5] + (r[5] - nv * math.sin(ph) / (beta * beta),)
+        if e["L"] > 0.0:
+            r = drift(r, e["L"] / 2.0, beti)
+        return r
+    if kind == "SOLENOID":  # tracking.jl:529-570
+        ks, L = e["param"][0], e["L"]
+        if ks == 0.0:
+            return drift(r, L, beti)
+        x, px, y, py, z, d = r
+        pn = 1.0 / (1.0 + d)
+        xpr, ypr = px * pn, py * pn
+        H = ks * pn / 2.0
+        S, C = math.sin(L * H), math.cos(L * H)
+        xn = x * C * C + xpr * C * S / H + y * C * S + ypr * S * S / H
+        pxn = (-x * H * C * S + xpr * C * C - y * H * S * S + ypr * C * S) / pn
+        yn = -x * C * S - xpr * S * S / H + y * C * C + ypr * C * S / H
+        pyn = (x * H * S * S - xpr * C * S - y * C * S * H + ypr * C * C) / pn
+        zn = z + L * (H * H * (x * x + y * y) + 2.0 * H * (xpr * y - ypr * x) + xpr * xpr + ypr * ypr) / 2.0
+        return (xn, pxn, yn, pyn, zn, d)
+    if kind == "CORRECTOR":  # tracking.jl:579-607
+        xk, yk = e["param"][0], e["param"][1]
+        x, px, y, py, z, d = r
+        pn = 1.0 / (1.0 + d)
+        nl = e["L"] * pn
+        zn = z + nl * pn * (xk * xk / 3.0 + yk * yk / 3.0 + px * px + py * py + px * xk + py * yk) / 2.0
+        return (x + nl * (px + xk / 2.0), px + xk, y + nl * (py + yk / 2.0), py + yk, zn, d)
+    if kind == "TRANSLATION":  # tracking.jl:1182-1192
+        x, px, y, py, z, d = r
+        dx, dy, ds = e["param"][0], e["param"][1], e["param"][2]
+        pz2 = 1.0 + 2.0 * d * beti + d * d - px * px - py * py
+        if pz2 <= 0.0:
+            return nan6()
+        pz = math.sqrt(pz2)
+        return (x - (dx + ds * px / pz), px, y - (dy + ds * py / pz), py, z + ds * (beti + d) / pz, d)
+    if kind == "YROTATION":  # tracking.jl:1194-1218
+        ang = -e["angle"]
+        if ang == 0.0:
+            return r
+        x, px, y, py, z, d = r
+        ca, sa, ta = math.cos(ang), math.sin(ang), math.tan(ang)
+        pz2 = 1.0 + 2.0 * d * beti + d * d - px * px - py * py
+        if pz2 <= 0.0:
+            return nan6()
+        pz = math.sqrt(pz2)
+        ptt = 1.0 - ta * px / pz
+        if abs(ptt) < math.sqrt(EPS):
+            return nan6()
+        return (x / (ca * ptt), ca * px + sa * pz, y + ta * x * py / (pz * ptt), py,
+                z + ta * x * (beti + d) / (pz * ptt), d)
+    if kind == "CRAB_CAVITY":  # tracking.jl:1531-1547
+        k, phi0, er1, er2 = e["param"][0], e["param"][1], e["param"][2], e["param"][3]
+        volt = e["volt"] * (1.0 + er1)
+        phi = phi0 + er2
+        E = max(abs(e["energy"]), EPS)
+        ang = k * r[4] + phi
+        if e["L"] > 0.0:
+            r = drift(r, e["L"] / 2.0, beti)
+        pxn = r[1] + (volt / E) * math.sin(ang * beti)
+        dn = r[5] - (k * volt / E * beti) * r[0] * math.cos(ang * beti)
+        r = (r[0], pxn, r[2], r[3], r[4], dn)
+        if e["L"] > 0.0:
+            r = drift(r, e["L"] / 2.0, beti)
+        return r
+    if kind == "ACCEL_CAVITY":  # tracking.jl:1549-1559
+        beta = 1.0 / beti
+        b2 = beta * beta
+        if b2 <= EPS:
+            return r
+        E = max(abs(e["energy"]), EPS)
+        k, phis = e["param"][0], e["param"][1]
+        sv = math.sin(k * r[4] + phis) - math.sin(phis)
+        return r[:5] + (r[5] + (e["volt"] / (b2 * E)) * sv,)
+    if kind == "LONGITUDINAL_RF_MAP":  # tracking.jl:1575-1585
+        alphac, k, h = e["param"][0], e["param"][1], e["param"][2]
+        if abs(k) <= EPS:
+            return r
+        beta = 1.0 / beti
+        eta = alphac - (1.0 - beta * beta)
+        return r[:4] + (r[4] - (TWO_PI * h * eta / k) * r[5], r[5])
+    if kind == "LORENTZ_BOOST":  # tracking.jl:1587-1595
+        if e["iparam"][0] != 0:
+            return r
+        ic = 1.0 / e["param"][1]
+        ta = e["param"][3]
+        return (r[0] + ta * r[4], r[1] * ic, r[2], r[3] * ic, r[4] * ic, r[5] - ta * r[1])
+    if kind == "INV_LORENTZ_BOOST":  # tracking.jl:1597-1604
+        if e["iparam"][0] != 0:
+            return r
+        c, s = e["param"][1], e["param"][2]
+        return (r[0] - s * r[4], r[1] * c, r[2], r[3] * c, r[4] * c, r[5] + s * r[1])
+    if kind == "STRONG_THIN_GAUSSIAN_BEAM":  # tracking.jl:1610-1619
+        amp, sx, sy, xo, yo = e["param"][:5]
+        sx2, sy2 = max(sx * sx, EPS), max(sy * sy, EPS)
+        dx, dy = r[0] - xo, r[2] - yo
+        g = amp * math.exp(-0.5 * (dx * dx / sx2 + dy * dy / sy2))
+        return (r[0], r[1] - g * dx / sx2, r[2], r[3] - g * dy / sy2, r[4], r[5])
+    raise ValueError(kind)
+
+
+def ringpass(elems, parts, beti, nturns=1, aperture=(0.0, 0.0)):
+    """ringpass!/linepass! (lattice.jl:260-317) on a list of particles."""
+    coords = [tuple(p) for p in parts]
+    lost = [0] * len(coords)
+    lost_turn = [-1] * len(coords)
+    lost_elem = [-1] * len(coords)
+    ax, ay = aperture
+    for t in range(nturns):
+        for ie, e in enumerate(elems):
+            for i in range(len(coords)):
+                if lost[i] == 1:
+                    continue
+                rn = apply_pass(e, coords[i], beti)
+                out = lost_check(rn) or (ax > 0.0 and abs(rn[0]) > ax) or (ay > 0.0 and abs(rn[2]) > ay)
+                if out:
+                    lost[i], lost_turn[i], lost_elem[i] = 1, t, ie
+                    continue
+                coords[i] = rn
+    return coords, lost, lost_turn, lost_elem
+
+
+def hexify(rows):
+    return [[float(v).hex() for v in row] for row in rows]
+
+
+def case(name, elems, parts, energy, nturns=1, aperture=(0.0, 0.0)):
+    beti = beti_of(energy)
+    out, lost, lt, le = ringpass(elems, parts, beti, nturns, aperture)
+    return dict(name=name, energy=energy, beti=beti.hex(), nturns=nturns, aperture=list(aperture),
+                elements=elems, input=hexify(parts), output=hexify(out), lost=lost, lost_turn=lt, lost_elem=le)
+
+
+def element_cases(energy):
+    """test/verify_elements.jl:52-118 (cases this engine supports)."""
+    acc = AccelCavity(0.0, volt=2.5e6, freq=500.0e6, h=1200.0, phis=0.2, energy=energy)
+    return [
+        ("Marker", [Marker()]),
+        ("Drift", [Drift(0.7)]),
+        ("Quadrupole", [Quadrupole(0.4, 1.3, num_int_steps=10)]),
+        ("Sextupole", [Sextupole(0.4, 2.0, num_int_steps=10)]),
+        ("Octupole", [Octupole(0.4, -3.0, num_int_steps=10)]),
+        ("ThinMultipole", [ThinMultipole(0.0, [0.0] * 4, [0.0, 0.2, -0.1, 0.05], max_order=3)]),
+        ("SBend", [SBend(0.9, 0.15, 0.03, 0.02, num_int_steps=10)]),
+        ("RBend", [RBend(0.9, 0.15, num_int_steps=10)]),
+        ("ExactSBend", [ExactSBend(0.9, 0.15, 0.03, 0.02, num_int_steps=10)]),
+        ("ERBend", [ERBend(0.9, 0.15, num_int_steps=10)]),
+        ("RFCavity", [RFCavity(0.3, 2.0e6, 500.0e6, 0.002, h=1200.0, philag=0.3, energy=energy)]),
+        ("CrabCavity", [CrabCavity(0.3, volt=2.0e6, freq=500.0e6, phi=0.1, energy=energy)]),
+        ("AccelCavity", [acc]),
+        ("LongitudinalRFMap", [LongitudinalRFMap(2.0e-4, acc)]),
+        ("Solenoid", [Solenoid(0.5, 0.8)]),
+        ("Corrector", [Corrector(0.4, 1.5e-4, -2.2e-4)]),
+        ("HKicker", [Corrector(0.0, 2.5e-4, 0.0)]),
+        ("VKicker", [Corrector(0.0, 0.0, -1.5e-4)]),
+        ("Translation", [Translation(0.0, dx=1e-3, dy=-2e-3, ds=3e-3)]),
+        ("YRotation", [YRotation(0.0, angle=0.02)]),
+        ("LorentzBoost", [LorentzBoost(0.03)]),
+        ("InvLorentzBoost", [InvLorentzBoost(0.03)]),
+        ("DriftSC", [DriftSC(0.5)]),
+        ("QuadrupoleSC", [QuadrupoleSC(0.4, k1=0.0)]),
+        ("SextupoleSC", [SextupoleSC(0.3, k2=2.4)]),
+        ("OctupoleSC", [OctupoleSC(0.2, k3=3.6)]),
+        ("SBendSC", [SBendSC(1.0, 0.0, 0.0, 0.0)]),
+        ("RBendSC", [SBendSC(1.2, 0.0, 0.0, 0.0)]),
+        ("SpaceCharge", [SpaceCharge(0.9)]),
+        ("StrongThinGaussianBeam", [StrongThinGaussianBeam(1.0e-6, 1.0e-3, 1.2e-3, 1.0e-4, -2.0e-4)]),
+    ]
+
+
+def extra_cases(energy):
+    """Cases beyond the reference suite: other edge methods, kick angles, skew terms."""
+    q = Quadrupole(0.5, -0.8)
+    q["kick_angle"] = [1.0e-4, -2.0e-4]
+    q["polynom_a"] = [0.0, 0.05, 0.0, 0.0]
+    sb2 = SBend(0.9, 0.15, 0.03, 0.02, fbe=2, fbx=3, fint1=0.5, fint2=0.4, gap=0.05)
+    sb2["polynom_b"] = [0.0, -0.3, 1.5, 0.0]
+    sb2["max_order"] = 2
+    eb = ExactSBend(1.5, 2.0 * math.pi / 40.0, math.pi / 40.0, math.pi / 40.0, gk=0.0)
+    eb_gk = ExactSBend(0.9, 0.15, 0.03, 0.02, gk=0.6)
+    eb_kick = ExactSBend(0.9, 0.15, 0.03, 0.02)
+    eb_kick["kick_angle"] = [1.0e-4, 5.0e-5]
+    eb0 = ExactSBend(0.9, 0.15, 0.03, 0.02, num_int_steps=0)
+    return [
+        ("QuadKickSkew", [q]),
+        ("SBendMethods23", [sb2]),
+        ("ExactSBendDBA", [eb]),
+        ("ExactSBendGK", [eb_gk]),
+        ("ExactSBendKick", [eb_kick]),
+        ("ExactSBendNoSteps", [eb0]),
+        ("RFNoEnergy", [RFCavity(0.2, 1.0e6, 500.0e6)]),
+    ]
+
+
+def fodo_line():  # test/verify_fodo.jl:30-39
+    return [Drift(1.0), Quadrupole(1.0, -0.9, num_int_steps=10), Drift(1.0), SBend(0.6, math.pi / 15.0),
+            Drift(1.0), Quadrupole(1.0, 0.3, num_int_steps=10), Drift(1.0)]
+
+
+def dba_line():  # test/verify_dba.jl:31-44
+    a = math.pi / 9
+    dl, ds = Drift(2.0), Drift(0.5)
+    b = SBend(1.0, a, a / 2, a / 2)
+    qf, qd = Quadrupole(0.4, 1.5), Quadrupole(0.4, -1.2)
+    return [dl, b, ds, qf, ds, qd, ds, qf, ds, b, dl]
+
+
+def fodo_ring():
+    """The FODO cell of the CPU workload: QF(0.5, +1.2) D(2.0) QD(0.5, -1.2) D(2.0), 8 cells."""
+    cell = [Quadrupole(0.5, 1.2), Drift(2.0), Quadrupole(0.5, -1.2), Drift(2.0)]
+    return cell * 8
+
+
+def main():
+    energy = 3.5e9
+    parts = PARTICLES
+    cases = []
+    for name, elems in element_cases(energy) + extra_cases(energy):
+        cases.append(case(name, elems, parts, energy))
+    cases.append(case("FODO_line", fodo_line(), parts, energy))
+    cases.append(case("DBA_line", dba_line(), parts, energy))
+    cases.append(case("Bend_pi4", [SBend(1.0, math.pi / 4, math.pi / 8, math.pi / 8)], parts, energy))
+    cases.append(case("ExactBend_pi9", [ExactSBend(1.0, math.pi / 9, math.pi / 18, math.pi / 18)], parts, energy))
+    cases.append(case("FODO_ring_10turns", fodo_ring(), parts, 1.0e9, nturns=10, aperture=(0.05, 0.05)))
+    # Loss semantics: amplitudes scaled up so that some particles cross the
+    # aperture or the angle limit at different turns and elements.
+    big = [[v * s for v in p] for p, s in zip(parts, [1, 2, 4, 6, 8, 10, 12, 14, 1500, 8000])]
+    cases.append(case("FODO_ring_losses", fodo_ring(), big, 1.0e9, nturns=6, aperture=(0.01, 0.0075)))
+    # Sextupoles make the large amplitudes unstable over several turns.
+    cell = [Quadrupole(0.5, 1.2), Sextupole(0.2, 100.0), Drift(2.0), Quadrupole(0.5, -1.2),
+            Sextupole(0.2, -100.0), Drift(2.0)]
+    big = [[v * s for v in p] for p, s in zip(parts, range(1, 11))]
+    cases.append(case("FODO_sext_losses", cell * 8, big, 1.0e9, nturns=20, aperture=(0.02, 0.015)))
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden_cases.json"), "w") as f:
+        json.dump(dict(generator="tests/golden/make_golden.py", mass=M_ELECTRON, cases=cases), f, indent=1)
+    print("wrote", len(cases), "cases")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,253 @@
+"""GPU tracking against the oracle and the golden fixtures, through the C ABI.
+
+Tolerances (the north-star parity gates):
+  * 1e-12 relative (per coordinate, scaled by the column's largest magnitude)
+    after one pass / one turn;
+  * bit-exact for the strict build (no FMA contraction) on maps that call no
+    transcendental function;
+  * loss flags, turn and element of loss identical.
+"""
+import numpy as np
+import pytest
+
+import oracle_ref
+from conftest import col_rel_err, tp, unhex
+
+pytestmark = pytest.mark.gpu
+W = __import__("trackpad_b200.workloads", fromlist=["x"])
+
+# Cases whose maps call no transcendental function per particle (host-hoisted
+# constants only): the strict build must match the oracle bit for bit.
+NO_TRANSC = {"Marker", "Drift", "Quadrupole", "Sextupole", "Octupole", "ThinMultipole", "SBend", "RBend",
+             "LongitudinalRFMap", "Corrector", "HKicker", "VKicker", "Translation", "YRotation", "LorentzBoost",
+             "InvLorentzBoost", "DriftSC", "QuadrupoleSC", "SextupoleSC", "OctupoleSC", "SBendSC", "RBendSC",
+             "SpaceCharge", "QuadKickSkew", "RFNoEnergy", "FODO_line", "DBA_line", "Bend_pi4", "FODO_ring_10turns",
+             "FODO_ring_losses", "FODO_sext_losses"}
+
+
+def _run_case(c, strict):
+    lat = tp.Lattice.from_records(c["elements"])
+    coords = np.asfortranarray(unhex(c["input"]))
+    n = coords.shape[0]
+    lost = np.zeros(n, np.int64)
+    lt = np.full(n, -1, np.int32)
+    le = np.full(n, -1, np.int32)
+    beam = tp.Beam(c["energy"])
+    tp.ringpass_(coords, lat, beam, lost, c["nturns"], aperture=tuple(c["aperture"]), lost_turn=lt, lost_elem=le,
+                 strict=strict)
+    return coords, lost, lt, le
+
+
+@pytest.mark.parametrize("strict", [False, True])
+def test_golden_cases(golden, strict):
+    for c in golden["cases"]:
+        coords, lost, lt, le = _run_case(c, strict)
+        ref = unhex(c["output"])
+        assert lost.tolist() == c["lost"], c["name"]
+        assert lt.tolist() == c["lost_turn"], c["name"]
+        assert le.tolist() == c["lost_elem"], c["name"]
+        if strict and c["name"] in NO_TRANSC:
+            assert np.array_equal(coords, ref), f"{c['name']}: strict build not bit-identical"
+        else:
+            err = col_rel_err(coords, ref)
+            assert err < 1e-12, f"{c['name']}: relative error {err}"
+
+
+def _compare(lat, beam, coords0, nturns, aperture, rtol, strict=False, **kw):
+    c = coords0.copy(order="F")
+    n = c.shape[0]
+    lost = np.zeros(n, np.int64)
+    lt = np.full(n, -1, np.int32)
+    le = np.full(n, -1, np.int32)
+    tp.ringpass_(c, lat, beam, lost, nturns, aperture=aperture, lost_turn=lt, lost_elem=le, strict=strict, **kw)
+    r = coords0.copy(order="F")
+    rl = np.zeros(n, np.int64)
+    rlt = np.full(n, -1, np.int32)
+    rle = np.full(n, -1, np.int32)
+    edge = np.full(n, np.inf)
+    oracle_ref.ringpass(lat, r, rl, tp.beti(beam), nturns, aperture=aperture, lost_turn=rlt, lost_elem=rle,
+                        min_edge=edge, exact=kw.get("exact", True))
+    # Loss bookkeeping must agree except for particles that came within 1e-10 of an edge.
+    mism = (lost != rl) | (lt != rlt) | (le != rle)
+    assert not (mism & (edge > 1e-10)).any(), f"{int(mism.sum())} loss mismatches away from the edges"
+    ok = (lost == 0) & (rl == 0)
+    if ok.any():
+        err = col_rel_err(c[ok], r[ok])
+        assert err < rtol, f"relative error {err}"
+    return c, lost, st_of()
+
+
+def st_of():
+    return tp.last_stats()
+
+
+def test_fodo_ring_cpu_workload():
+    """FODO ring on 1 GeV electrons: 10,000 Gaussian particles, 100 turns,
+    aperture 0.05 m (the CPU-runnable workload), against the oracle."""
+    lat, beam = W.fodo_ring(), W.fodo_beam()
+    coords = W.gaussian(10000, seed=0)
+    _, lost, st = _compare(lat, beam, coords, 100, 0.05, 1e-10)
+    assert st["particles"] == 10000 and st["units"] == 10000 * 32 * 100
+
+
+@pytest.mark.parametrize("strict", [False, True])
+def test_dba_one_turn(strict):
+    """DBA ring, one turn: 1e-12 relative (Gaussian core and a slice of the DA grid)."""
+    lat, beam = W.dba_ring(), W.dba_beam()
+    coords = np.asfortranarray(np.concatenate([W.gaussian(2048, seed=0), W.da_grid(32, 32)]))
+    _compare(lat, beam, coords, 1, 0.02, 1e-12, strict=strict)
+
+
+def test_dba_ten_turns_with_losses():
+    lat, beam = W.dba_ring(), W.dba_beam()
+    coords = np.asfortranarray(np.concatenate([W.gaussian(512, seed=1), W.da_grid(24, 24)]))
+    c, lost, st = _compare(lat, beam, coords, 10, 0.02, 1e-11)
+    assert 0 < lost.sum() < len(lost)
+    assert st["survivors"] == int((lost == 0).sum())
+
+
+@pytest.mark.parametrize("schedule", [1, 2])
+@pytest.mark.parametrize("block", [64, 128, 256])
+def test_schedules_and_blocks_agree_bitwise(schedule, block):
+    """Static and lane-refill scheduling at every block size give identical bits."""
+    lat, beam = W.dba_ring(cells=4), W.dba_beam()
+    coords0 = np.asfortranarray(np.concatenate([W.gaussian(3000, seed=2), W.da_grid(20, 20)]))
+    ref = coords0.copy(order="F")
+    rl = np.zeros(len(ref), np.int64)
+    tp.ringpass_(ref, lat, beam, rl, 5, aperture=0.02, schedule=1, block_size=128)
+    c = coords0.copy(order="F")
+    l = np.zeros(len(c), np.int64)
+    tp.ringpass_(c, lat, beam, l, 5, aperture=0.02, schedule=schedule, block_size=block)
+    assert np.array_equal(l, rl) and np.array_equal(c, ref)
+
+
+def test_ringpass_equals_repeated_linepass():
+    """ringpass!(n) == n x linepass! (src/lattice.jl:305-317)."""
+    lat, beam = W.dba_ring(cells=3), W.dba_beam()
+    c0 = np.asfortranarray(np.concatenate([W.gaussian(500, seed=4), W.da_grid(10, 10)]))
+    a = c0.copy(order="F")
+    la = np.zeros(len(a), np.int64)
+    tp.ringpass_(a, lat, beam, la, 4, aperture=0.02)
+    b = c0.copy(order="F")
+    lb = np.zeros(len(b), np.int64)
+    for t in range(4):
+        tp.linepass_(b, lat, beam, lb, turn=t, aperture=0.02)
+    assert np.array_equal(la, lb) and np.array_equal(a, b)
+
+
+def test_edge_cases():
+    lat, beam = W.fodo_ring(), W.fodo_beam()
+    # N = 0 and nturns = 0 are no-ops
+    tp.ringpass_(np.zeros((0, 6), order="F"), lat, beam, np.zeros(0, np.int64), 10)
+    c = W.gaussian(100, seed=5)
+    c0 = c.copy()
+    tp.ringpass_(c, lat, beam, np.zeros(100, np.int64), 0)
+    assert np.array_equal(c, c0)
+    # pre-lost particles are untouched; flags other than 1 count as alive
+    flags = np.array([1, 2] * 50, np.int64)
+    tp.ringpass_(c, lat, beam, flags, 3)
+    assert np.array_equal(c[0::2], c0[0::2]) and not np.array_equal(c[1::2], c0[1::2])
+    assert flags[1::2].tolist() == [2] * 50
+    # every particle lost on the first element keeps its input coordinates
+    big = np.asfortranarray(np.full((33, 6), 0.0))
+    big[:, 0] = 2.0
+    fl = np.zeros(33, np.int64)
+    tp.ringpass_(big, lat, beam, fl, 5)
+    assert fl.tolist() == [1] * 33 and (big[:, 0] == 2.0).all()
+    # ragged sizes
+    for n in (1, 31, 33, 257):
+        cc = W.gaussian(n, seed=n)
+        _compare(lat, beam, cc, 2, 0.05, 1e-12)
+
+
+def test_row_major_input_is_updated_in_place():
+    lat, beam = W.fodo_ring(cells=1), W.fodo_beam()
+    c = np.ascontiguousarray(W.gaussian(64, seed=6))
+    ref = np.asfortranarray(c)
+    tp.ringpass_(c, lat, beam, np.zeros(64, np.int64), 2)
+    oracle_ref.ringpass(lat, ref, np.zeros(64, np.int64), tp.beti(beam), 2)
+    assert col_rel_err(c, ref) < 1e-12
+
+
+def test_device_pointers_match_host_path():
+    import torch
+    lat, beam = W.dba_ring(cells=2), W.dba_beam()
+    host = W.gaussian(4096, seed=7)
+    dev = torch.from_numpy(np.ascontiguousarray(host.T)).cuda()  # (6, N) rows = columns of the N x 6 matrix
+    lost_d = torch.zeros(4096, dtype=torch.int64, device="cuda")
+    tp.ringpass_(dev.T, lat, beam, lost_d, 3, aperture=0.02)
+    lost_h = np.zeros(4096, np.int64)
+    tp.ringpass_(host, lat, beam, lost_h, 3, aperture=0.02)
+    torch.cuda.synchronize()
+    assert np.array_equal(dev.cpu().numpy().T, host) and np.array_equal(lost_d.cpu().numpy(), lost_h)
+
+
+def test_linearised_drift_option():
+    lat, beam = W.fodo_ring(cells=2), W.fodo_beam()
+    c = W.gaussian(256, seed=8)
+    _compare(lat, beam, c, 3, 0.05, 1e-12, exact=False)
+
+
+def test_time_dependent_schedule():
+    """timed quadrupole k1 and RF voltage, evaluated per turn (as materialize
+    does per linepass! call), against the oracle with the same per-turn values."""
+    import math
+    base = W.dba_ring(cells=2)
+    elems = list(base.elements)
+    qi = next(i for i, e in enumerate(elems) if e.kind == "QUADRUPOLE")
+    ri = len(elems) - 1
+    elems[qi] = tp.timed(elems[qi], k1=lambda ctx, k0=elems[qi].k1: k0 * (1 + 0.01 * ctx.turn / 20))
+    elems[ri] = tp.timed(elems[ri], volt=lambda ctx, v0=elems[ri].volt: v0 * (1 + 0.05 * math.sin(2 * math.pi * ctx.turn / 200)))
+    lat = tp.Lattice(elems)
+    beam = W.dba_beam()
+    c0 = W.gaussian(300, seed=9)
+    c = c0.copy(order="F")
+    lost = np.zeros(300, np.int64)
+    tp.ringpass_(c, lat, beam, lost, 6, turn=3, aperture=0.02)
+    vals = np.array([[elems[qi].updates["k1"](tp.TimeContext(0.0, t)), elems[ri].updates["volt"](tp.TimeContext(0.0, t))]
+                     for t in range(3, 9)])
+    r = c0.copy(order="F")
+    rl = np.zeros(300, np.int64)
+    oracle_ref.ringpass(base, r, rl, tp.beti(beam), 6, turn0=3, aperture=0.02,
+                        sched=([qi, 1, ri, 5], 3, vals))
+    assert np.array_equal(lost, rl)
+    assert col_rel_err(c, r) < 1e-12
+
+
+def test_batched_equals_lattice_by_lattice():
+    """One ragged batched launch == each variant tracked on its own, bit for bit."""
+    variants = W.dba_variants(nvar=6, seed=3, n_base=300)
+    batch = tp.Batch([v for v, _ in variants])
+    beam = W.dba_beam()
+    counts = [n for _, n in variants]
+    poff = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    coords = np.asfortranarray(np.concatenate([W.gaussian(n, seed=10 + i) for i, n in enumerate(counts)]))
+    ref = coords.copy(order="F")
+    lost = np.zeros(len(coords), np.int64)
+    for use_graph in (False, True, True):
+        c = coords.copy(order="F")
+        l = np.zeros(len(c), np.int64)
+        batch.ringpass_(c, poff, np.full(len(counts), tp.beti(beam)), l, 4, aperture=0.02, use_graph=use_graph)
+        for i, (lat, n) in enumerate(variants):
+            s = slice(poff[i], poff[i + 1])
+            rc = np.asfortranarray(ref[s])
+            rl = np.zeros(n, np.int64)
+            tp.ringpass_(rc, lat, beam, rl, 4, aperture=0.02, schedule=1)
+            assert np.array_equal(c[s], rc) and np.array_equal(l[s], rl)
+    st = tp.last_stats()
+    assert st["units"] == sum(n * len(v) * 4 for v, n in variants)
+
+
+def test_unsupported_schedule_outside_range():
+    base = W.dba_ring(cells=1)
+    elems = list(base.elements)
+    elems[1] = tp.timed(elems[1], k1=lambda ctx: 1.0)
+    lat = tp.Lattice(elems)
+    lat.set_schedule(0.0, 0.0, 0, 2)
+    c = W.gaussian(10, seed=1)
+    import ctypes as C
+    o = tp.tracking._opts(None, True, False, False)
+    st = tp._abi.lib().tp_ringpass(tp.context(), lat.handle, c.ctypes.data_as(C.c_void_p), 10,
+                                   np.zeros(10, np.int64).ctypes.data_as(C.c_void_p), None, None,
+                                   C.c_double(1.0001), 5, C.c_double(0), C.c_double(0), 0, C.byref(o))
+    assert st == tp._abi.TP_ERANGE

@@ -1,0 +1,16 @@
+"""trackpad_b200 -- B200 multi-particle tracking engine for TrackPad.jl.
+
+The package directory is `trackpad.jl_b200/`; load it under the module name
+`trackpad_b200` (see `load()` in the repository's entry scripts).  The public
+names mirror TrackPad.jl (`linepass!` -> `linepass_`, `ringpass!` -> `ringpass_`).
+"""
+from . import _abi
+from .elements import (AbstractElement, AccelCavity, Corrector, CrabCavity, Drift, DriftSC, ERBend, ExactSBend,
+                       HKicker, InvLorentzBoost, LongitudinalRFMap, LorentzBoost, M_ELECTRON, M_PROTON, Marker,
+                       Octupole, OctupoleSC, Quadrupole, QuadrupoleSC, RBend, RBendSC, RFCavity, SBend, SBendSC,
+                       Sextupole, SextupoleSC, Solenoid, SpaceCharge, StrongThinGaussianBeam, ThinMultipole,
+                       Translation, VKicker, YRotation)
+from .tracking import (Batch, Beam, Lattice, Time, TimeContext, TimeDependentParam, TimeVaryingElement, Turn, beti,
+                       context, last_stats, linepass_, materialize, probe_fp64_peak, ringpass_, spos, timed)
+
+__all__ = [n for n in dir() if not n.startswith("_")]

@@ -1,0 +1,475 @@
+// tp_compile.cpp -- validation of tp_elem records and their compilation into
+// the device element program (tp_program.h), plus the algorithmic FLOP model.
+//
+// Host constants are computed with the operations, operands and order the
+// reference uses per particle (built with -ffp-contract=off), so hoisting them
+// out of the particle loop does not change a single bit of the result.
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "tp_internal.h"
+
+namespace tp {
+
+namespace {
+
+constexpr double DRIFT1 = 0.6756035959798286638;   // src/tracking.jl:29-32
+constexpr double DRIFT2 = -0.1756035959798286639;
+constexpr double KICK1 = 1.351207191959657328;
+constexpr double KICK2 = -1.702414383919314656;
+constexpr double TWO_PI = 6.283185307179586;        // Float64(2pi)
+constexpr double EPS = 2.220446049250313e-16;       // eps(Float64)
+
+// Julia max(a, b) for Float64 with b = eps: NaN propagates.
+double jmax_eps(double a) { return std::isnan(a) ? a : (a < EPS ? EPS : a); }
+
+bool has_misalign_fields(int kind) {
+    switch (kind) {
+        case TP_DRIFT: case TP_DRIFT_SC: case TP_QUADRUPOLE: case TP_SEXTUPOLE: case TP_OCTUPOLE:
+        case TP_THIN_MULTIPOLE: case TP_SBEND: case TP_EXACT_SBEND: case TP_SOLENOID: case TP_CORRECTOR:
+        case TP_QUADRUPOLE_SC: case TP_SEXTUPOLE_SC: case TP_OCTUPOLE_SC: case TP_SBEND_SC:
+            return true;
+        default:
+            return false;
+    }
+}
+
+bool uses_order(int kind) {
+    switch (kind) {
+        case TP_QUADRUPOLE: case TP_SEXTUPOLE: case TP_OCTUPOLE: case TP_THIN_MULTIPOLE: case TP_SBEND:
+        case TP_EXACT_SBEND:
+            return true;
+        default:
+            return false;
+    }
+}
+
+struct Rec {
+    RecHdr h{};
+    double w[MAX_REC_WORDS]{};
+    int nw = 0;  // payload words
+};
+
+// symplectic4_pass / symplectic4_bend_pass slice constants (src/tracking.jl:325-329).
+void yoshida_consts(double L, int n, double* L1, double* L2, double* K1, double* K2) {
+    double SL = L / double(n);
+    *L1 = SL * DRIFT1;
+    *L2 = SL * DRIFT2;
+    *K1 = SL * KICK1;
+    *K2 = SL * KICK2;
+}
+
+// kick_angle folding (src/tracking.jl:396-411, 668-682, 931-940).
+void fold_kick(const tp_elem& e, double* pa, double* pb) {
+    if (e.L > 0.0) {
+        pb[0] = pb[0] - std::sin(e.kick_angle[0]) / e.L;
+        pa[0] = pa[0] + std::sin(e.kick_angle[1]) / e.L;
+    }
+}
+
+}  // namespace
+
+int validate_elem(const tp_elem& e, int64_t idx, int64_t nmis, std::string* err) {
+    auto fail = [&](const char* what) {
+        *err = "element " + std::to_string(idx) + ": " + what;
+        return TP_EINVAL;
+    };
+    if (e.kind < 0 || e.kind >= TP_KIND_COUNT) {
+        *err = "element " + std::to_string(idx) + ": unknown kind " + std::to_string(e.kind);
+        return TP_EUNSUPPORTED;
+    }
+    if (uses_order(e.kind) && (e.max_order < 0 || e.max_order > 3))
+        return fail("max_order must be in 0..3 (polynom_a/polynom_b hold 4 coefficients)");
+    if (e.misalign_index >= 0) {
+        if (!has_misalign_fields(e.kind)) return fail("this element kind has no misalignment fields");
+        if (e.misalign_index >= nmis) return fail("misalign_index out of range");
+    } else if (e.misalign_index != -1) {
+        return fail("misalign_index must be -1 or a row index");
+    }
+    return TP_OK;
+}
+
+// Compile one element.  Returns the record words (header + payload).
+static Rec compile_rec(const tp_elem& e) {
+    Rec r;
+    r.h.kind = DK_IDENTITY;
+    r.h.order = 0;
+    r.h.nsteps = e.num_int_steps;
+    r.h.aux = -1;
+    if (e.misalign_index >= 0 && has_misalign_fields(e.kind)) {
+        r.h.flags |= RF_MISALIGN;
+        r.h.aux = e.misalign_index;
+    }
+    switch (e.kind) {
+        case TP_MARKER:
+        case TP_SPACE_CHARGE:
+            r.h.kind = DK_IDENTITY;
+            break;
+        case TP_DRIFT:
+        case TP_DRIFT_SC:
+            r.h.kind = DK_DRIFT;
+            r.w[drift::L] = e.L;
+            r.nw = drift::WORDS;
+            break;
+        case TP_QUADRUPOLE: case TP_SEXTUPOLE: case TP_OCTUPOLE:
+        case TP_QUADRUPOLE_SC: case TP_SEXTUPOLE_SC: case TP_OCTUPOLE_SC: {
+            double pa[4], pb[4];
+            for (int i = 0; i < 4; ++i) { pa[i] = e.polynom_a[i]; pb[i] = e.polynom_b[i]; }
+            int order = e.max_order;
+            if (e.kind == TP_QUADRUPOLE) {            // tracking.jl:394-411
+                pb[1] = e.k;
+                fold_kick(e, pa, pb);
+            } else if (e.kind == TP_SEXTUPOLE) {      // tracking.jl:446
+                pb[2] = e.k / 2.0;
+            } else if (e.kind == TP_OCTUPOLE) {       // tracking.jl:478
+                pb[3] = e.k / 6.0;
+            } else {                                   // _sc_polynom_b, tracking.jl:993-995
+                pb[0] = e.param[0]; pb[1] = e.param[1]; pb[2] = e.param[2] / 2.0; pb[3] = e.param[3] / 6.0;
+                if (e.kind == TP_QUADRUPOLE_SC) fold_kick(e, pa, pb);
+                order = order < 0 ? 0 : (order > 3 ? 3 : order);
+            }
+            r.h.kind = DK_MULTIPOLE;
+            r.h.order = uint8_t(order);
+            yoshida_consts(e.L, e.num_int_steps, &r.w[mp::L1], &r.w[mp::L2], &r.w[mp::K1], &r.w[mp::K2]);
+            for (int i = 0; i < 4; ++i) { r.w[mp::PA + i] = pa[i]; r.w[mp::PB + i] = pb[i]; }
+            r.nw = mp::WORDS;
+            break;
+        }
+        case TP_THIN_MULTIPOLE:
+            r.h.kind = DK_THIN;
+            r.h.order = uint8_t(e.max_order);
+            for (int i = 0; i < 4; ++i) { r.w[thin::PA + i] = e.polynom_a[i]; r.w[thin::PB + i] = e.polynom_b[i]; }
+            r.nw = thin::WORDS;
+            break;
+        case TP_SBEND:
+        case TP_SBEND_SC: {
+            if (e.kind == TP_SBEND_SC && e.L == 0.0) {  // tracking.jl:1047-1049
+                r.h.kind = DK_NAN;
+                break;
+            }
+            int order = e.max_order;
+            if (e.kind == TP_SBEND_SC) order = order < 0 ? 0 : (order > 3 ? 3 : order);
+            double irho = e.angle / e.L;
+            double pa[4], pb[4];
+            for (int i = 0; i < 4; ++i) { pa[i] = e.polynom_a[i]; pb[i] = e.polynom_b[i]; }
+            fold_kick(e, pa, pb);
+            r.h.kind = DK_SBEND;
+            r.h.order = uint8_t(order);
+            yoshida_consts(e.L, e.num_int_steps, &r.w[mp::L1], &r.w[mp::L2], &r.w[mp::K1], &r.w[mp::K2]);
+            for (int i = 0; i < 4; ++i) { r.w[mp::PA + i] = pa[i]; r.w[mp::PB + i] = pb[i]; }
+            r.w[sb::IRHO] = irho;
+            // edge_fringe_entrance / _exit constants (tracking.jl:162-172, 196-206)
+            auto edge = [&](int method, double ang, double fint, double* fx, double* eang, double* fc) {
+                double corr;
+                if (fint == 0.0 || e.gap == 0.0 || method == 0) {
+                    corr = 0.0;
+                } else {
+                    double sedge = std::sin(ang), cedge = std::cos(ang);
+                    corr = irho * e.gap * fint * (1.0 + sedge * sedge) / cedge;
+                }
+                *fx = irho * std::tan(ang);
+                *eang = ang;
+                *fc = corr;
+            };
+            if (e.fringe_bend_entrance != 0) {
+                r.h.flags |= RF_FRINGE_IN;
+                r.h.method_in = uint8_t(e.fringe_bend_entrance >= 1 && e.fringe_bend_entrance <= 3
+                                            ? e.fringe_bend_entrance : 1);
+                edge(e.fringe_bend_entrance, e.e1, e.fint1, &r.w[sb::FX_IN], &r.w[sb::E_IN], &r.w[sb::FC_IN]);
+                if (r.w[sb::FC_IN] == 0.0) r.h.flags |= RF_FC_IN_ZERO;
+            }
+            if (e.fringe_bend_exit != 0) {
+                r.h.flags |= RF_FRINGE_OUT;
+                r.h.method_out = uint8_t(e.fringe_bend_exit >= 1 && e.fringe_bend_exit <= 3 ? e.fringe_bend_exit : 1);
+                edge(e.fringe_bend_exit, e.e2, e.fint2, &r.w[sb::FX_OUT], &r.w[sb::E_OUT], &r.w[sb::FC_OUT]);
+                if (r.w[sb::FC_OUT] == 0.0) r.h.flags |= RF_FC_OUT_ZERO;
+            }
+            r.nw = sb::WORDS;
+            break;
+        }
+        case TP_EXACT_SBEND: {  // tracking.jl:901-973
+            double irho = e.angle / e.L;
+            r.h.kind = DK_EXACT_SBEND;
+            r.h.order = uint8_t(e.max_order);
+            r.w[eb::IRHO] = irho;
+            r.w[eb::GK] = e.gk;
+            if (e.e1 != 0.0) {
+                r.h.flags |= RF_YROT_IN;
+                r.w[eb::YC_IN] = std::cos(e.e1);
+                r.w[eb::YS_IN] = std::sin(e.e1);
+            }
+            if (e.e2 != 0.0) {
+                r.h.flags |= RF_YROT_OUT;
+                r.w[eb::YC_OUT] = std::cos(e.e2);
+                r.w[eb::YS_OUT] = std::sin(e.e2);
+            }
+            if (e.fringe_bend_entrance != 0) r.h.flags |= RF_FRINGE_IN;
+            if (e.fringe_bend_exit != 0) r.h.flags |= RF_FRINGE_OUT;
+            if (!(std::fabs(irho) < 1e-6)) {
+                r.h.flags |= RF_EDGE;  // bend_edge returns r unchanged when |rhoinv| < 1e-6
+                double t_in = -e.e1, t_out = -e.e2;
+                r.w[eb::EC_IN] = std::cos(t_in);
+                r.w[eb::ES_IN] = std::sin(t_in);
+                r.w[eb::ES2_IN] = std::sin(2.0 * t_in);
+                r.w[eb::ETH_IN] = t_in;
+                r.w[eb::ETHH_IN] = t_in / irho;
+                r.w[eb::EC_OUT] = std::cos(t_out);
+                r.w[eb::ES_OUT] = std::sin(t_out);
+                r.w[eb::ES2_OUT] = std::sin(2.0 * t_out);
+                r.w[eb::ETH_OUT] = t_out;
+                r.w[eb::ETHH_OUT] = t_out / irho;
+            } else {
+                r.h.flags |= RF_STRAIGHT;  // exact_bend_body drift limit
+            }
+            if (e.num_int_steps == 0) {
+                r.h.flags |= RF_BODY_ONE;
+                r.w[eb::L1] = e.L;
+                r.w[eb::CS1] = std::cos(irho * e.L);
+                r.w[eb::SN1] = std::sin(irho * e.L);
+            } else {
+                double pa[4], pb[4];
+                for (int i = 0; i < 4; ++i) { pa[i] = e.polynom_a[i]; pb[i] = e.polynom_b[i]; }
+                fold_kick(e, pa, pb);
+                yoshida_consts(e.L, e.num_int_steps, &r.w[eb::L1], &r.w[eb::L2], &r.w[eb::K1], &r.w[eb::K2]);
+                r.w[eb::CS1] = std::cos(irho * r.w[eb::L1]);
+                r.w[eb::SN1] = std::sin(irho * r.w[eb::L1]);
+                r.w[eb::CS2] = std::cos(irho * r.w[eb::L2]);
+                r.w[eb::SN2] = std::sin(irho * r.w[eb::L2]);
+                for (int i = 0; i < 4; ++i) { r.w[eb::PA + i] = pa[i]; r.w[eb::PB + i] = pb[i]; }
+                // With max_order 0 the kick is px -= K*pb[0], py += K*pa[0]: exact no-ops
+                // when both coefficients are zero (only the sign of a zero can change).
+                if (e.max_order == 0 && pb[0] == 0.0 && pa[0] == 0.0) r.h.flags |= RF_NOKICK;
+            }
+            r.nw = eb::WORDS;
+            break;
+        }
+        case TP_RFCAVITY:  // tracking.jl:502-518
+            r.h.kind = DK_RF;
+            if (e.L > 0.0) { r.h.flags |= RF_LPOS; r.w[rf::LH] = e.L / 2.0; }
+            if (e.energy > 0.0) {
+                r.h.flags |= RF_ENERGY;
+                r.w[rf::NV] = e.volt / e.energy;
+                r.w[rf::W] = TWO_PI * e.freq;
+                r.w[rf::LAG] = e.lag;
+                r.w[rf::PHILAG] = e.philag;
+            }
+            r.nw = rf::WORDS;
+            break;
+        case TP_SOLENOID:
+            r.h.kind = DK_SOLENOID;
+            r.w[sol::L] = e.L;
+            r.w[sol::KS] = e.param[0];
+            r.nw = sol::WORDS;
+            break;
+        case TP_CORRECTOR:
+            r.h.kind = DK_CORRECTOR;
+            r.w[cor::L] = e.L;
+            r.w[cor::XK] = e.param[0];
+            r.w[cor::YK] = e.param[1];
+            r.nw = cor::WORDS;
+            break;
+        case TP_TRANSLATION:
+            r.h.kind = DK_TRANSLATION;
+            r.w[trn::DX] = e.param[0];
+            r.w[trn::DY] = e.param[1];
+            r.w[trn::DS] = e.param[2];
+            r.nw = trn::WORDS;
+            break;
+        case TP_YROTATION: {  // tracking.jl:1194-1218
+            double angle = -e.angle;
+            if (angle == 0.0) { r.h.kind = DK_IDENTITY; break; }
+            r.h.kind = DK_YROTATION;
+            r.w[yr::CA] = std::cos(angle);
+            r.w[yr::SA] = std::sin(angle);
+            r.w[yr::TA] = std::tan(angle);
+            r.nw = yr::WORDS;
+            break;
+        }
+        case TP_CRAB_CAVITY:  // tracking.jl:1531-1547
+            r.h.kind = DK_CRAB;
+            if (e.L > 0.0) { r.h.flags |= RF_LPOS; r.w[crab::LH] = e.L / 2.0; }
+            r.w[crab::VOLT] = e.volt * (1.0 + e.param[2]);
+            r.w[crab::PHI] = e.param[1] + e.param[3];
+            r.w[crab::E] = jmax_eps(std::fabs(e.energy));
+            r.w[crab::K] = e.param[0];
+            r.nw = crab::WORDS;
+            break;
+        case TP_ACCEL_CAVITY:  // tracking.jl:1549-1559
+            r.h.kind = DK_ACCEL;
+            r.w[acc::VOLT] = e.volt;
+            r.w[acc::E] = jmax_eps(std::fabs(e.energy));
+            r.w[acc::K] = e.param[0];
+            r.w[acc::PHIS] = e.param[1];
+            r.w[acc::SINPHIS] = std::sin(e.param[1]);
+            r.nw = acc::WORDS;
+            break;
+        case TP_LONGITUDINAL_RF_MAP:  // tracking.jl:1575-1585
+            if (std::fabs(e.param[1]) <= EPS) { r.h.kind = DK_IDENTITY; break; }
+            r.h.kind = DK_LONG_RF_MAP;
+            r.w[lrf::ALPHAC] = e.param[0];
+            r.w[lrf::K] = e.param[1];
+            r.w[lrf::H] = e.param[2];
+            r.nw = lrf::WORDS;
+            break;
+        case TP_LORENTZ_BOOST:  // tracking.jl:1587-1595
+            if (e.iparam[0] != 0) { r.h.kind = DK_IDENTITY; break; }
+            r.h.kind = DK_LORENTZ;
+            r.w[lor::A] = 1.0 / e.param[1];
+            r.w[lor::B] = e.param[3];
+            r.nw = lor::WORDS;
+            break;
+        case TP_INV_LORENTZ_BOOST:  // tracking.jl:1597-1604
+            if (e.iparam[0] != 0) { r.h.kind = DK_IDENTITY; break; }
+            r.h.kind = DK_INV_LORENTZ;
+            r.w[lor::A] = e.param[1];
+            r.w[lor::B] = e.param[2];
+            r.nw = lor::WORDS;
+            break;
+        case TP_STRONG_THIN_GAUSSIAN_BEAM: {  // tracking.jl:1610-1619
+            r.h.kind = DK_STRONG_THIN_GAUSS;
+            double sx2 = e.param[1] * e.param[1], sy2 = e.param[2] * e.param[2];
+            r.w[stg::AMP] = e.param[0];
+            r.w[stg::SX2] = jmax_eps(sx2);
+            r.w[stg::SY2] = jmax_eps(sy2);
+            r.w[stg::XO] = e.param[3];
+            r.w[stg::YO] = e.param[4];
+            r.nw = stg::WORDS;
+            break;
+        }
+        default:
+            break;
+    }
+    r.h.words = uint16_t(HDR_WORDS + r.nw);
+    return r;
+}
+
+static void append_rec(const Rec& r, std::vector<double>* out) {
+    size_t at = out->size();
+    out->resize(at + r.h.words);
+    std::memcpy(out->data() + at, &r.h, sizeof(RecHdr));
+    for (int i = 0; i < r.nw; ++i) (*out)[at + HDR_WORDS + i] = r.w[i];
+}
+
+void compile_record(const tp_elem& e, std::vector<double>* out) { append_rec(compile_rec(e), out); }
+
+int record_words(const tp_elem& e) { return compile_rec(e).h.words; }
+
+void scheduled_stub(const tp_elem& e, int32_t slot, std::vector<double>* out) {
+    Rec r;
+    r.h.kind = compile_rec(e).h.kind;
+    r.h.flags = RF_SCHEDULED;
+    r.h.words = HDR_WORDS;
+    r.h.aux = slot;
+    append_rec(r, out);
+}
+
+void apply_field(tp_elem* e, int field, double v) {
+    switch (field) {
+        case TP_FIELD_L: e->L = v; break;
+        case TP_FIELD_K: e->k = v; break;
+        case TP_FIELD_ANGLE: e->angle = v; break;
+        case TP_FIELD_E1: e->e1 = v; break;
+        case TP_FIELD_E2: e->e2 = v; break;
+        case TP_FIELD_VOLT: e->volt = v; break;
+        case TP_FIELD_FREQ: e->freq = v; break;
+        case TP_FIELD_LAG: e->lag = v; break;
+        case TP_FIELD_PHILAG: e->philag = v; break;
+        case TP_FIELD_ENERGY: e->energy = v; break;
+        case TP_FIELD_NUM_INT_STEPS: e->num_int_steps = int32_t(v); break;
+        default:
+            if (field >= TP_FIELD_POLYNOM_A0 && field < TP_FIELD_POLYNOM_A0 + 4)
+                e->polynom_a[field - TP_FIELD_POLYNOM_A0] = v;
+            else if (field >= TP_FIELD_POLYNOM_B0 && field < TP_FIELD_POLYNOM_B0 + 4)
+                e->polynom_b[field - TP_FIELD_POLYNOM_B0] = v;
+            break;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Algorithmic FLOP model: operations the reference's pass! performs for one
+// typical particle, counted with add/sub/mul/div/sqrt = 1 and each
+// transcendental call = TP_FLOPS_PER_TRANSCENDENTAL (20).  Every constant
+// below is checked against the oracle's op-counting scalar in the CPU tests.
+// ---------------------------------------------------------------------------
+double elem_flops(const tp_elem& e, const tp_misalign* mis, bool exact) {
+    const double TR = TP_FLOPS_PER_TRANSCENDENTAL;
+    const double D = exact ? 20.0 : 14.0;           // drift6
+    auto kick = [](int m) { return 8.0 * m + 4.0; };  // strthinkick
+    auto bkick = [](int m) { return 8.0 * m + 12.0; };  // bndthinkick
+    double mis_f = 0.0;
+    if (has_misalign_fields(e.kind)) {
+        mis_f = 12.0;  // r + t1, r + t2 are always evaluated
+        if (mis) {
+            bool r1 = false, r2 = false;
+            for (int i = 0; i < 36; ++i) { r1 |= mis->r1[i] != 0.0; r2 |= mis->r2[i] != 0.0; }
+            mis_f += (r1 ? 66.0 : 0.0) + (r2 ? 66.0 : 0.0);
+        }
+    }
+    const int n = e.num_int_steps > 0 ? e.num_int_steps : 0;
+    const double fold = e.L > 0.0 ? 4.0 + 2.0 * TR : 0.0;
+    switch (e.kind) {
+        case TP_MARKER: case TP_SPACE_CHARGE: return 0.0;
+        case TP_DRIFT: case TP_DRIFT_SC: return mis_f + D;
+        case TP_QUADRUPOLE:
+            return mis_f + fold + 5.0 + n * (4.0 * D + 3.0 * kick(e.max_order));
+        case TP_SEXTUPOLE: case TP_OCTUPOLE:
+            return mis_f + 1.0 + 5.0 + n * (4.0 * D + 3.0 * kick(e.max_order));
+        case TP_QUADRUPOLE_SC: case TP_SEXTUPOLE_SC: case TP_OCTUPOLE_SC: {
+            int m = e.max_order < 0 ? 0 : (e.max_order > 3 ? 3 : e.max_order);
+            return mis_f + 2.0 + (e.kind == TP_QUADRUPOLE_SC ? fold : 0.0) + 5.0 + n * (4.0 * D + 3.0 * kick(m));
+        }
+        case TP_THIN_MULTIPOLE: return mis_f + kick(e.max_order);
+        case TP_SBEND: case TP_SBEND_SC: {
+            if (e.kind == TP_SBEND_SC && e.L == 0.0) return mis_f;
+            int m = e.max_order;
+            if (e.kind == TP_SBEND_SC) m = m < 0 ? 0 : (m > 3 ? 3 : m);
+            auto edge = [&](int method, double fint) {
+                if (method == 0) return 0.0;
+                double f = 49.0;
+                if (!(fint == 0.0 || e.gap == 0.0)) f += 46.0;  // sin, cos and the fringecorr product
+                if (method == 2) f += 2.0;
+                if (method == 3) f += 1.0;
+                return f;
+            };
+            return mis_f + 1.0 + fold + 5.0 + edge(e.fringe_bend_entrance, e.fint1) +
+                   n * (4.0 * D + 3.0 * bkick(m)) + edge(e.fringe_bend_exit, e.fint2);
+        }
+        case TP_EXACT_SBEND: {
+            const double body = 124.0, yrot = 63.0, fringe = 243.0, edge = 152.0;
+            double f = mis_f + 1.0;
+            if (e.e1 != 0.0) f += yrot;
+            if (e.e2 != 0.0) f += yrot;
+            if (e.fringe_bend_entrance != 0) f += fringe;
+            if (e.fringe_bend_exit != 0) f += fringe;
+            double irho = e.angle / e.L;
+            if (!(std::fabs(irho) < 1e-6)) f += 2.0 * edge;
+            if (e.num_int_steps == 0) {
+                f += body;
+            } else {
+                f += 5.0 + fold + n * (4.0 * body + 3.0 * kick(e.max_order));
+            }
+            return f;
+        }
+        case TP_RFCAVITY: {
+            double f = 1.0;
+            if (e.L > 0.0) f += 2.0 * (1.0 + D);
+            if (e.energy > 0.0) f += 30.0;
+            return f;
+        }
+        case TP_SOLENOID: return mis_f + (e.param[0] == 0.0 ? D : 80.0 + 2.0 * TR);
+        case TP_CORRECTOR: return mis_f + 30.0;
+        case TP_TRANSLATION: return 22.0;
+        case TP_YROTATION: return e.angle == 0.0 ? 0.0 : 29.0 + 3.0 * TR;
+        case TP_CRAB_CAVITY: return 16.0 + 2.0 * TR + (e.L > 0.0 ? 2.0 * (1.0 + D) : 0.0);
+        case TP_ACCEL_CAVITY: return 9.0 + 2.0 * TR;
+        case TP_LONGITUDINAL_RF_MAP: return 9.0;
+        case TP_LORENTZ_BOOST: return 8.0;
+        case TP_INV_LORENTZ_BOOST: return 7.0;
+        case TP_STRONG_THIN_GAUSSIAN_BEAM: return 17.0 + TR;
+        default: return 0.0;
+    }
+}
+
+}  // namespace tp

@@ -1,0 +1,70 @@
+// tp_internal.h -- declarations shared by the library's translation units.
+#pragma once
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/trackpad_b200.h"
+#include "tp_program.h"
+
+namespace tp {
+
+// Host compiler (tp_compile.cpp)
+int validate_elem(const tp_elem& e, int64_t idx, int64_t nmis, std::string* err);
+void compile_record(const tp_elem& e, std::vector<double>* out);
+int record_words(const tp_elem& e);
+void scheduled_stub(const tp_elem& e, int32_t slot, std::vector<double>* out);
+void apply_field(tp_elem* e, int field, double v);
+double elem_flops(const tp_elem& e, const tp_misalign* mis, bool exact);
+
+// Arguments of one tracking launch.  All pointers are device pointers.
+struct TrackArgs {
+    const double* table;        // compiled program, `table_words` words (16-byte multiple)
+    int32_t table_words;
+    int32_t nelem;
+    const double* sched;        // per-turn records of scheduled elements (may be null)
+    int32_t sched_stride;       // words per turn block
+    int32_t sched_turn0;
+    int32_t sched_nturns;
+    int32_t pad0;
+    const MisalignDev* mis;
+    double* coords;             // N x 6 column-major
+    int64_t n;
+    int64_t* lost_flags;
+    int32_t* lost_turn;         // may be null
+    int32_t* lost_elem;         // may be null
+    double beti;
+    double limx, limy;          // loss limits on |x|, |y|: min(1, aperture)
+    int32_t nturns;
+    int32_t turn0;
+    int32_t exact;              // exact Hamiltonian drift
+    int32_t refill;             // lane-refill scheduling
+    unsigned long long* work;   // refill counter (scratch, zeroed by the host)
+    unsigned long long* passes; // particle-element maps evaluated (scratch, zeroed)
+    int32_t* err;               // device error word (scratch, zeroed)
+    // Batched (ragged) launches: variant v owns particles [poff[v], poff[v+1])
+    // and program words [toff[v], toff[v+1]).  nvar == 0 for single lattices.
+    const int64_t* poff;
+    const int64_t* toff;
+    const double* beti_v;
+    const int32_t* nelem_v;
+    int32_t nvar;
+    int32_t smem_words;         // words staged into shared memory per block
+};
+
+// Device error word bits.
+enum DevErr : int32_t {
+    DE_BAD_KIND = 1,
+    DE_SCHED_RANGE = 2,
+    DE_TMA_TIMEOUT = 4,
+};
+
+// Kernel launchers (tp_track.cu, compiled once with and once without FMA
+// contraction).  Return a cudaError_t value.
+int launch_track_fast(const TrackArgs& a, int grid, int block, int ppt, size_t smem, void* stream);
+int launch_track_strict(const TrackArgs& a, int grid, int block, int ppt, size_t smem, void* stream);
+int occupancy_track_fast(int block, int ppt, size_t smem, int* blocks_per_sm);
+int occupancy_track_strict(int block, int ppt, size_t smem, int* blocks_per_sm);
+
+}  // namespace tp

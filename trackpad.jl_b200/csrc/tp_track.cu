@@ -1,0 +1,313 @@
+// tp_track.cu -- the tracking kernel (ringpass!/linepass! on the device).
+//
+// One thread per particle; the 6D FP64 state stays in registers across every
+// element and turn of the launch.  The compiled element table is staged into
+// shared memory once per block with a TMA bulk copy (cp.async.bulk, no
+// multicast) completed on an mbarrier; every lane of a warp then reads the
+// same record (broadcast).  Particles are read and written in coalesced SoA
+// order (column c of the N x 6 column-major array).
+//
+// Scheduling.  With lane refill a persistent warp takes particle indices from
+// a global counter (one warp-aggregated atomic per refill); a lane whose
+// particle is lost or finished takes the next particle at the next turn
+// boundary, so loss does not leave lanes idle for the rest of the launch.
+// Every particle is still tracked from turn 0 with its own turn counter, so
+// the result is the same as the reference's loop order.  Static scheduling
+// gives each thread one particle.  Batched launches hand out 32-particle
+// tiles of (variant, particles) and read each variant's table through L1.
+//
+// This file is compiled twice: with FMA contraction (TP_NS = fast) and
+// without (-fmad=false, TP_NS = strict, bit-identical arithmetic to the
+// oracle except inside transcendental calls).
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "tp_internal.h"
+#include "tp_maps.cuh"
+
+#ifndef TP_NS
+#define TP_NS fast
+#endif
+
+namespace tp {
+namespace TP_NS {
+
+using namespace tp::dev;
+
+constexpr int kMaxBlock = 256;
+constexpr long long kTmaSpinLimit = 1ll << 22;  // bounded mbarrier wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Stage `words` words of the element table into shared memory with
+// cp.async.bulk (global -> shared::cluster, which for a launch without
+// clusters is this CTA's own shared memory) completed on an mbarrier.
+// Returns false if the bounded wait ran out.
+__device__ bool stage_table(double* dst, const double* src, int words, uint64_t* mbar) {
+    const uint32_t bar = smem_u32(mbar);
+    const uint32_t bytes = uint32_t(words) * 8u;  // multiple of 16: the host pads the table
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        const uint32_t chunk = 32768u;
+        for (uint32_t off = 0; off < bytes; off += chunk) {
+            uint32_t n = bytes - off < chunk ? bytes - off : chunk;
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_u32(reinterpret_cast<char*>(dst) + off)),
+                "l"(reinterpret_cast<const char*>(src) + off), "r"(n), "r"(bar)
+                : "memory");
+        }
+    }
+    uint32_t done = 0;
+    long long spins = 0;
+    while (!done) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(0u)
+            : "memory");
+        if (++spins > kTmaSpinLimit) break;
+    }
+    __syncthreads();
+    return done != 0;
+}
+
+__device__ __forceinline__ void load_state(const double* coords, int64_t n, int64_t i, P6& s) {
+    s.x = coords[i];
+    s.px = coords[n + i];
+    s.y = coords[2 * n + i];
+    s.py = coords[3 * n + i];
+    s.z = coords[4 * n + i];
+    s.d = coords[5 * n + i];
+}
+
+__device__ __forceinline__ void store_state(double* coords, int64_t n, int64_t i, const P6& s) {
+    coords[i] = s.x;
+    coords[n + i] = s.px;
+    coords[2 * n + i] = s.y;
+    coords[3 * n + i] = s.py;
+    coords[4 * n + i] = s.z;
+    coords[5 * n + i] = s.d;
+}
+
+// check_lost (src/tracking.jl:49-52) fused with the rectangular aperture:
+// |x| > 1 or |x| > ax  <=>  |x| > min(1, ax).
+__device__ __forceinline__ bool is_lost(const P6& s, double limx, double limy) {
+    return isnan(s.x) || fabs(s.x) > limx || fabs(s.y) > limy || fabs(s.px) > 1.0 || fabs(s.py) > 1.0;
+}
+
+// Header of the record to use at `turn` (scheduled elements live in the
+// per-turn table).  Returns null when the turn is outside the schedule.
+__device__ __forceinline__ const double* resolve(const double* rec, RecHdr& h, const TrackArgs& a, int turn) {
+    if (!(h.flags & RF_SCHEDULED)) return rec;
+    int row = turn - a.sched_turn0;
+    if (row < 0 || row >= a.sched_nturns) return nullptr;
+    const double* p = a.sched + int64_t(row) * a.sched_stride + h.aux;
+    h = *reinterpret_cast<const RecHdr*>(p);
+    return p;
+}
+
+// Track the particles of one warp through `nturns` turns of the table `tab`
+// (`nelem` records).  Slot state is per lane.  With REFILL, lanes take new
+// particles from `next_particle` at turn boundaries until it returns < 0.
+template <bool EXACT, bool REFILL, typename NextFn>
+__device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, double beti, NextFn next_particle,
+                         unsigned long long& passes) {
+    const double beta = 1.0 / beti;
+    const double beta2 = beta * beta;
+    const int lane = threadIdx.x & 31;
+    P6 s{};
+    int64_t idx = -1;
+    int t = 0;
+    bool act = false;
+    bool more = true;  // warp-uniform: the particle source is not exhausted
+
+    for (;;) {
+        // Refill empty lanes at the turn boundary.
+        while (more) {
+            unsigned need = __ballot_sync(0xffffffffu, !act);
+            if (need == 0) break;
+            int64_t j = next_particle(need, lane, more);
+            if (!act && j >= 0) {
+                if (a.lost_flags[j] != 1) {
+                    load_state(a.coords, a.n, j, s);
+                    idx = j;
+                    t = 0;
+                    act = true;
+                }
+            }
+            if (!REFILL) more = false;
+        }
+        if (__ballot_sync(0xffffffffu, act) == 0) {
+            if (!more) break;
+            continue;
+        }
+        // One turn.
+        const double* rec = tab;
+        for (int e = 0; e < nelem; ++e) {
+            RecHdr h0 = *reinterpret_cast<const RecHdr*>(rec);
+            const double* next = rec + h0.words;
+            unsigned live = __ballot_sync(0xffffffffu, act);
+            if (live == 0) break;  // every lane of this warp is empty: skip the rest of the turn
+            if (lane == 0) passes += __popc(live);
+            if (act) {
+                RecHdr h = h0;
+                const double* r = resolve(rec, h, a, a.turn0 + t);
+                if (r == nullptr) {
+                    atomicOr(a.err, DE_SCHED_RANGE);
+                    act = false;
+                } else {
+                    P6 sn = s;
+                    if (!apply_record<EXACT>(sn, r, h, a.mis, beti, beta, beta2)) {
+                        atomicOr(a.err, DE_BAD_KIND);
+                        act = false;
+                    } else if (is_lost(sn, a.limx, a.limy)) {
+                        // linepass!: flag the particle, keep the entrance coordinates
+                        // (src/lattice.jl:281-284).
+                        store_state(a.coords, a.n, idx, s);
+                        a.lost_flags[idx] = 1;
+                        if (a.lost_turn) a.lost_turn[idx] = a.turn0 + t;
+                        if (a.lost_elem) a.lost_elem[idx] = e;
+                        act = false;
+                    } else {
+                        s = sn;
+                    }
+                }
+            }
+            rec = next;
+        }
+        if (act) {
+            ++t;
+            if (t == a.nturns) {
+                store_state(a.coords, a.n, idx, s);
+                act = false;
+            }
+        }
+    }
+}
+
+template <bool EXACT, bool REFILL>
+__global__ void __launch_bounds__(kMaxBlock) track_single(TrackArgs a) {
+    extern __shared__ __align__(16) double smem[];
+    __shared__ __align__(8) uint64_t mbar;
+    const double* tab = a.table;
+    if (a.smem_words > 0) {
+        if (!stage_table(smem, a.table, a.smem_words, &mbar)) {
+            if (threadIdx.x == 0) atomicOr(a.err, DE_TMA_TIMEOUT);
+            return;
+        }
+        tab = smem;
+    }
+    unsigned long long passes = 0;
+    if (REFILL) {
+        auto next = [&](unsigned need, int lane, bool& more) -> int64_t {
+            unsigned long long base = 0;
+            int cnt = __popc(need);
+            if (lane == 0) base = atomicAdd(a.work, (unsigned long long)cnt);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + (unsigned long long)cnt >= (unsigned long long)a.n) more = false;
+            if (!((need >> lane) & 1u)) return -1;
+            unsigned long long j = base + __popc(need & ((1u << lane) - 1u));
+            return j < (unsigned long long)a.n ? int64_t(j) : -1;
+        };
+        run_warp<EXACT, true>(a, tab, a.nelem, a.beti, next, passes);
+    } else {
+        const int64_t gid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+        auto next = [&](unsigned need, int lane, bool& more) -> int64_t {
+            more = false;
+            return gid < a.n ? gid : -1;
+        };
+        run_warp<EXACT, false>(a, tab, a.nelem, a.beti, next, passes);
+    }
+    if ((threadIdx.x & 31) == 0 && passes) atomicAdd(a.passes, passes);
+}
+
+// Batched: warps take 32-particle tiles (variant, first particle) in variant
+// order; tile t of variant v covers particles poff[v] + 32*(t - tile_off[v]).
+template <bool EXACT>
+__global__ void __launch_bounds__(kMaxBlock) track_batched(TrackArgs a, const int64_t* tile_off) {
+    const int lane = threadIdx.x & 31;
+    unsigned long long passes = 0;
+    const int64_t ntiles = tile_off[a.nvar];
+    for (;;) {
+        unsigned long long tile = 0;
+        if (lane == 0) tile = atomicAdd(a.work, 1ull);
+        tile = __shfl_sync(0xffffffffu, tile, 0);
+        if (tile >= (unsigned long long)ntiles) break;
+        // variant of this tile: last v with tile_off[v] <= tile
+        int lo = 0, hi = a.nvar - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if (tile_off[mid] <= (int64_t)tile) lo = mid; else hi = mid - 1;
+        }
+        const int v = lo;
+        const int64_t first = a.poff[v] + 32 * (int64_t(tile) - tile_off[v]);
+        const int64_t endp = a.poff[v + 1];
+        const int64_t mine = first + lane;
+        auto next = [&](unsigned need, int ln, bool& more) -> int64_t {
+            more = false;
+            return mine < endp ? mine : -1;
+        };
+        run_warp<EXACT, false>(a, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next, passes);
+    }
+    if (lane == 0 && passes) atomicAdd(a.passes, passes);
+}
+
+static size_t smem_bytes(const TrackArgs& a) { return size_t(a.smem_words) * 8; }
+
+int launch(const TrackArgs& a, int grid, int block, int ppt, size_t smem, void* stream) {
+    (void)ppt;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (a.nvar > 0) {
+        const int64_t* tile_off = a.toff + (a.nvar + 1);  // host packs tile offsets after toff
+        if (a.exact) track_batched<true><<<grid, block, 0, st>>>(a, tile_off);
+        else track_batched<false><<<grid, block, 0, st>>>(a, tile_off);
+        return int(cudaGetLastError());
+    }
+    (void)smem_bytes;
+    if (smem > 48 * 1024) {
+        cudaError_t e;
+        if (a.exact && a.refill) e = cudaFuncSetAttribute(track_single<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        else if (a.exact) e = cudaFuncSetAttribute(track_single<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        else if (a.refill) e = cudaFuncSetAttribute(track_single<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        else e = cudaFuncSetAttribute(track_single<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return int(e);
+    }
+    if (a.exact && a.refill) track_single<true, true><<<grid, block, smem, st>>>(a);
+    else if (a.exact) track_single<true, false><<<grid, block, smem, st>>>(a);
+    else if (a.refill) track_single<false, true><<<grid, block, smem, st>>>(a);
+    else track_single<false, false><<<grid, block, smem, st>>>(a);
+    return int(cudaGetLastError());
+}
+
+int occupancy(int block, int ppt, size_t smem, int* blocks_per_sm) {
+    (void)ppt;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(track_single<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return int(e);
+    }
+    return int(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, track_single<true, true>, block, smem));
+}
+
+}  // namespace TP_NS
+
+#define TP_CAT2(a, b) a##_##b
+#define TP_CAT(a, b) TP_CAT2(a, b)
+int TP_CAT(launch_track, TP_NS)(const TrackArgs& a, int grid, int block, int ppt, size_t smem, void* stream) {
+    return TP_NS::launch(a, grid, block, ppt, smem, stream);
+}
+int TP_CAT(occupancy_track, TP_NS)(int block, int ppt, size_t smem, int* blocks_per_sm) {
+    return TP_NS::occupancy(block, ppt, smem, blocks_per_sm);
+}
+
+}  // namespace tp
