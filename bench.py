@@ -39,7 +39,7 @@ def parse():
     p.add_argument("--workload", default="dba", choices=["dba", "fodo", "batched"])
     p.add_argument("--n-gauss", type=int, default=1 << 20)
     p.add_argument("--grid", type=int, default=512)
-    p.add_argument("--strict", action="store_true")
+    p.add_argument("--contract", action="store_true", help="kernels built with FMA contraction")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
@@ -112,7 +112,8 @@ def workload(args, rank):
 def cpu_baseline(w, target_s=10.0, chunk=1024, threads=0):
     """The oracle (C++ restatement of the reference loop order: elements outer,
     particles inner, OpenMP over particles) on the host cores, on successive
-    1-turn chunks of the workload's own beam until about `target_s` seconds."""
+    chunks of the workload's own beam, each tracked over the step's turns, until
+    about `target_s` seconds."""
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import oracle_ref
     import trackpad_b200 as tp
@@ -126,13 +127,13 @@ def cpu_baseline(w, target_s=10.0, chunk=1024, threads=0):
         c = np.asfortranarray(w["coords"][idx])
         lost = np.zeros(len(c), np.int64)
         t0 = time.perf_counter()
-        oracle_ref.ringpass(lat, c, lost, tp.beti(beam), 1, aperture=w["aperture"], nthreads=nthreads)
+        oracle_ref.ringpass(lat, c, lost, tp.beti(beam), w["turns"], aperture=w["aperture"], nthreads=nthreads)
         dt += time.perf_counter() - t0
-        units += float(len(c)) * len(lat)
+        units += float(len(c)) * len(lat) * w["turns"]
         chunks += 1
     return {"value": units / dt, "unit": "particle*element*turns/s", "cores": nthreads, "kind": "port",
-            "sample": f"{chunks} x {chunk} particles drawn from the workload's beam, 1 turn each, "
-                      f"OpenMP over particles, {dt:.1f} s"}
+            "sample": f"{chunks} x {chunk} particles drawn from the workload's beam, {w['turns']} turns each "
+                      f"(one step), OpenMP over particles, {dt:.1f} s"}
 
 
 def run_reference(args):
@@ -155,7 +156,7 @@ def run_reference(args):
             "unit": "particle*element*turns/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 4000.0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Philox Gaussian beam + DA grid)",
-            "config": {"workload": w["name"], "step": "about 4 s of 1-turn chunks of the beam per step"},
+            "config": {"workload": w["name"], "step": f"about 4 s of {w['turns']}-turn chunks of the beam per step"},
             "cpu_baseline": {"value": v, "unit": base["unit"], "cores": base["cores"], "kind": "port",
                              "sample": base["sample"]},
             "e2e": {"value": v, "unit": "particle*element*turns/s", "h2d_bytes_per_step": 0,
@@ -195,7 +196,7 @@ def main():
         coords.copy_(init)
         lost.zero_()
         tp.ringpass_(coords.T, lat, beam, lost, turns, aperture=aperture, lost_turn=lost_turn, lost_elem=lost_elem,
-                     strict=args.strict, stream=sptr)
+                     contract=args.contract, stream=sptr)
         st = tp.last_stats(local)
         flush.fill_(1)  # L2 flush between timed iterations
         return st
@@ -273,7 +274,7 @@ def main():
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox Gaussian beam + DA grid)",
             "config": {"workload": w["name"], "turns_per_step": turns, "particles_per_gpu": n,
                        "elements": len(lat), "l2": "flushed between timed steps (256 MiB write)",
-                       "fp": "strict (no FMA contraction)" if args.strict else "FMA contraction"},
+                       "fp": "FMA contraction" if args.contract else "no FMA contraction (reference operation order)"},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": None,
                          "peak_source": "measured FP64 FMA throughput of this device (tp_probe_fp64_peak)",

@@ -154,7 +154,10 @@ typedef struct tp_opts {
                                   reference global USE_EXACT_HAMILTONIAN,
                                   tracking.jl:38,100-107                          */
     int32_t device_pointers;   /* 1: data pointers are device pointers            */
-    int32_t fp_strict;         /* 1: kernels built without FMA contraction         */
+    int32_t fp_contract;       /* 1: use the kernels built with FMA contraction.
+                                  Default 0: no contraction, so every map evaluates
+                                  the reference's operations in its order (exact
+                                  bends amplify a changed rounding to ~1e-11)     */
     int32_t block_size;        /* threads per block; 0 = autotuned                */
     int32_t ppt;               /* particles per thread (1 or 2); 0 = autotuned    */
     int32_t schedule;          /* 0 = autotuned, 1 = static, 2 = lane refill      */
@@ -180,7 +183,7 @@ typedef struct tp_stats {
     int32_t grid;
     int32_t launches;          /* kernels this library launched in the call      */
     int32_t schedule;          /* 1 = static, 2 = lane refill                      */
-    int32_t fp_strict;
+    int32_t fp_contract;
 } tp_stats;
 
 /* ------------------------------------------------------------------------- */

@@ -32,6 +32,7 @@
 #include <vector>
 
 #include "../include/trackpad_b200.h"
+#include "../trackpad.jl_b200/csrc/tp_libm.h"
 
 namespace tpo {
 
@@ -49,10 +50,18 @@ constexpr double M_ELECTRON = 0.51099895069e6;
 constexpr double TWO_PI = 6.283185307179586;  // Float64(2pi)
 constexpr double EPS = 2.220446049250313e-16; // eps(Float64)
 
-// Scalar helpers.  For double these are the libm calls; other scalar types
-// provide overloads found by argument-dependent lookup.
+// Scalar helpers.  sin, cos, tan, asin and atan of a double come from
+// tp_libm.h: the published fdlibm method in explicitly rounded IEEE operations,
+// the implementation the CUDA kernels use, so that the oracle and the device
+// evaluate the same function (both within 1 ulp of the C library).  Other
+// scalar types provide overloads found by argument-dependent lookup.
 inline double value_of(double x) { return x; }
 inline bool is_nan(double x) { return std::isnan(x); }
+inline double sin(double x) { return tp::libm::sin(x); }
+inline double cos(double x) { return tp::libm::cos(x); }
+inline double tan(double x) { return tp::libm::tan(x); }
+inline double asin(double x) { return tp::libm::asin(x); }
+inline double atan(double x) { return tp::libm::atan(x); }
 
 template <class T>
 struct V6 {
@@ -193,7 +202,6 @@ inline V6<T> pass_drift(const Elem<T>& e, V6<T> r, T beti, bool exact) {
 // ---------------------------------------------------------------------------
 template <class T>
 inline V6<T> edge_fringe(const V6<T>& r, T inv_rho, T edge_angle, T fint, T gap, int method, bool is_exit) {
-    using std::cos; using std::sin; using std::tan;
     T fringecorr;
     if (value_of(fint) == 0.0 || value_of(gap) == 0.0 || method == 0) {
         fringecorr = T(0.0);
@@ -301,7 +309,6 @@ inline V6<T> symplectic4_bend_pass(V6<T> r, T L, const T* pa, const T* pb, T irh
 // ExactSBend (:931-940), QuadrupoleSC (:1004-1007), SBendSC (:1052-1055).
 template <class T>
 inline void fold_kick_angle(const Elem<T>& e, T* pa, T* pb) {
-    using std::sin;
     if (value_of(e.L) > 0.0) {
         pb[0] = pb[0] - sin(e.kick[0]) / e.L;
         pa[0] = pa[0] + sin(e.kick[1]) / e.L;
@@ -340,7 +347,6 @@ inline V6<T> pass_oct(const Elem<T>& e, V6<T> r, T beti, bool exact) {
 // pass!(::RFCavity): src/tracking.jl:502-518
 template <class T>
 inline V6<T> pass_rf(const Elem<T>& e, V6<T> r, T beti, bool exact) {
-    using std::sin;
     T beta = T(1.0) / beti;
     if (value_of(e.L) > 0.0) r = drift6(r, e.L / T(2.0), beti, exact);
     if (value_of(e.energy) > 0.0) {
@@ -356,7 +362,6 @@ inline V6<T> pass_rf(const Elem<T>& e, V6<T> r, T beti, bool exact) {
 // pass!(::Solenoid): src/tracking.jl:529-570
 template <class T>
 inline V6<T> pass_solenoid(const Elem<T>& e, V6<T> r, T beti, bool exact) {
-    using std::cos; using std::sin;
     r = entrance(e, r);
     T ks = e.param[0];
     T L = e.L;
@@ -451,7 +456,6 @@ inline T clamp1(T x) {
 
 template <class T>
 inline V6<T> yrot(const V6<T>& r, T phi, T beti) {
-    using std::cos; using std::sin;
     if (value_of(phi) == 0.0) return r;
     T dp1 = beti + r[5];
     T c = cos(phi);
@@ -467,8 +471,7 @@ inline V6<T> yrot(const V6<T>& r, T phi, T beti) {
 
 template <class T>
 inline V6<T> bend_fringe(const V6<T>& r, T irho, T gK, T beti) {
-    using std::atan; using std::cos; using std::sqrt; using std::tan;
-    T b0 = irho;
+    using std::sqrt; T b0 = irho;
     T dp1 = beti + r[5];
     T pz = pxyz(dp1, r[1], r[3]);
     T px = r[1];
@@ -522,8 +525,7 @@ inline V6<T> bend_fringe(const V6<T>& r, T irho, T gK, T beti) {
 
 template <class T>
 inline V6<T> bend_edge(const V6<T>& r, T rhoinv, T theta, T beti) {
-    using std::abs; using std::asin; using std::cos; using std::sin;
-    if (value_of(abs(rhoinv)) < 1e-6) return r;
+    using std::abs; if (value_of(abs(rhoinv)) < 1e-6) return r;
     T dp1 = beti + r[5];
     T c = cos(theta);
     T s = sin(theta);
@@ -543,8 +545,7 @@ inline V6<T> bend_edge(const V6<T>& r, T rhoinv, T theta, T beti) {
 
 template <class T>
 inline V6<T> exact_bend_body(const V6<T>& r, T irho, T L, T beti) {
-    using std::abs; using std::asin; using std::cos; using std::sin;
-    T dp1 = beti + r[5];
+    using std::abs; T dp1 = beti + r[5];
     T pz = pxyz(dp1, r[1], r[3]);
     if (value_of(abs(irho)) < 1e-6) {
         T NormL = L / pz;
@@ -638,8 +639,7 @@ inline V6<T> pass_translation(const Elem<T>& e, const V6<T>& r, T beti) {
 // YRotation: src/tracking.jl:1194-1218
 template <class T>
 inline V6<T> pass_yrotation(const Elem<T>& e, const V6<T>& r, T beti) {
-    using std::abs; using std::cos; using std::sin; using std::sqrt; using std::tan;
-    T angle = -e.angle;
+    using std::abs; using std::sqrt; T angle = -e.angle;
     if (value_of(angle) == 0.0) return r;
     T ca = cos(angle);
     T sa = sin(angle);
@@ -659,8 +659,7 @@ inline V6<T> pass_yrotation(const Elem<T>& e, const V6<T>& r, T beti) {
 // CrabCavity: src/tracking.jl:1531-1547
 template <class T>
 inline V6<T> pass_crab(const Elem<T>& e, V6<T> r, T beti, bool exact) {
-    using std::abs; using std::cos; using std::sin;
-    T volt = e.volt * (T(1.0) + e.param[2]);
+    using std::abs; T volt = e.volt * (T(1.0) + e.param[2]);
     T phi = e.param[1] + e.param[3];
     T E = abs(e.energy);
     if (value_of(E) < EPS || is_nan(E)) E = is_nan(E) ? E : T(EPS);  // max(abs(energy), eps)
@@ -677,8 +676,7 @@ inline V6<T> pass_crab(const Elem<T>& e, V6<T> r, T beti, bool exact) {
 // AccelCavity: src/tracking.jl:1549-1559
 template <class T>
 inline V6<T> pass_accel(const Elem<T>& e, const V6<T>& r, T beti) {
-    using std::abs; using std::sin;
-    T beta = T(1.0) / beti;
+    using std::abs; T beta = T(1.0) / beti;
     T beta2 = beta * beta;
     if (value_of(beta2) <= EPS) return r;
     T E = abs(e.energy);

@@ -3,8 +3,9 @@
 An independent pure-Python transcription of TrackPad.jl's per-particle maps
 (src/tracking.jl) and of linepass!/ringpass! (src/lattice.jl:260-317), written
 separately from the C++ oracle so that the two transcriptions check each other.
-Python floats are IEEE binary64 with no fused multiply-add and `math` calls the
-C library, so the oracle must reproduce these numbers bit for bit.
+Python floats are IEEE binary64 with no fused multiply-add; sin, cos, tan, asin
+and atan come from fdlibm_py (the published fdlibm method, the one the kernels
+and the oracle implement), so the oracle must reproduce these numbers bit for bit.
 
 The cases are the reference's own parity tests, run on its own 10-particle
 fixture (test/verify_elements.jl:10-21, energy 3.5e9 eV):
@@ -20,6 +21,10 @@ Usage:  python tests/golden/make_golden.py   (writes golden_*.json here)
 import json
 import math
 import os
+import sys
+
+sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+import fdlibm_py as fm  # noqa: E402
 
 NAN = float("nan")
 COORD_LIMIT = 1.0  # tracking.jl:25
@@ -159,11 +164,11 @@ def LongitudinalRFMap(alphac, rf):  # _rf_k/_rf_h: tracking.jl:1565-1573
 
 
 def LorentzBoost(angle, mode=0):  # elements/beambeam.jl:14-19
-    return elem("LORENTZ_BOOST", param=[angle, math.cos(angle), 0.0, math.tan(angle)] + [0.0] * 4, iparam=[mode, 0])
+    return elem("LORENTZ_BOOST", param=[angle, fm.cos(angle), 0.0, fm.tan(angle)] + [0.0] * 4, iparam=[mode, 0])
 
 
 def InvLorentzBoost(angle, mode=0):  # elements/beambeam.jl:38-43
-    return elem("INV_LORENTZ_BOOST", param=[angle, math.cos(angle), math.sin(angle), 0.0] + [0.0] * 4,
+    return elem("INV_LORENTZ_BOOST", param=[angle, fm.cos(angle), fm.sin(angle), 0.0] + [0.0] * 4,
                 iparam=[mode, 0])
 
 
@@ -251,8 +256,8 @@ def yoshida(r, L, steps, drift_fn, kick_fn):  # tracking.jl:317-375
 def folded(e, pa, pb):  # kick_angle folding, tracking.jl:396-411
     pa, pb = list(pa), list(pb)
     if e["L"] > 0.0:
-        pb[0] = pb[0] - math.sin(e["kick_angle"][0]) / e["L"]
-        pa[0] = pa[0] + math.sin(e["kick_angle"][1]) / e["L"]
+        pb[0] = pb[0] - fm.sin(e["kick_angle"][0]) / e["L"]
+        pa[0] = pa[0] + fm.sin(e["kick_angle"][1]) / e["L"]
     return pa, pb
 
 
@@ -260,16 +265,16 @@ def edge(r, irho, ang, fint, gap, method, at_exit):  # tracking.jl:160-221
     if fint == 0.0 or gap == 0.0 or method == 0:
         fc = 0.0
     else:
-        se, ce = math.sin(ang), math.cos(ang)
+        se, ce = fm.sin(ang), fm.cos(ang)
         fc = irho * gap * fint * (1.0 + se * se) / ce
-    fx = irho * math.tan(ang)
+    fx = irho * fm.tan(ang)
     opd = 1.0 + r[5]
     if method == 2:
-        fy = irho * math.tan(ang - fc / opd) / opd
+        fy = irho * fm.tan(ang - fc / opd) / opd
     elif method == 3:
-        fy = irho * math.tan(ang - fc - r[1] / opd) if at_exit else irho * math.tan(ang - fc + r[1] / opd)
+        fy = irho * fm.tan(ang - fc - r[1] / opd) if at_exit else irho * fm.tan(ang - fc + r[1] / opd)
     else:
-        fy = irho * math.tan(ang - fc / opd)
+        fy = irho * fm.tan(ang - fc / opd)
     return (r[0], r[1] + r[0] * fx, r[2], r[3] - r[2] * fy, r[4], r[5])
 
 
@@ -287,7 +292,7 @@ def yrot(r, phi, beti):  # tracking.jl:727-745
         return r
     x, px, y, py, z, d = r
     dp1 = beti + d
-    c, s = math.cos(phi), math.sin(phi)
+    c, s = fm.cos(phi), fm.sin(phi)
     pz = pxyz(dp1, px, py)
     p = c * pz - s * px
     return (x * pz / p, s * pz + c * px, y + x * py * s / p, py, z + dp1 * x * s / p, d)
@@ -301,12 +306,12 @@ def fringe(r, irho, gk, beti):  # bend_fringe, tracking.jl:752-815
     xp, yp = px / pz, py / pz
     t1 = 1.0 + xp * xp * (2.0 + yp * yp)
     t2 = xp / (1.0 + yp * yp)
-    phi = -b0 * math.tan(b0 * gk * t1 * pz - math.atan(t2))
+    phi = -b0 * fm.tan(b0 * gk * t1 * pz - fm.atan(t2))
     px2, py2, pz2 = px * px, py * py, pz * pz
     pz4 = pz2 * pz2
     s2 = py2 + pz2
-    arg = (b0 * gk * (pz4 + px2 * (py2 + 2.0 * pz2))) / (pz2 * pz) - math.atan(px * pz / (py2 + pz2))
-    sec = 1.0 / math.cos(arg)
+    arg = (b0 * gk * (pz4 + px2 * (py2 + 2.0 * pz2))) / (pz2 * pz) - fm.atan(px * pz / (py2 + pz2))
+    sec = 1.0 / fm.cos(arg)
     psec = sec * sec
     py4 = py2 * py2
     py6 = py4 * py2
@@ -336,12 +341,12 @@ def wedge(r, h, theta, beti):  # bend_edge, tracking.jl:822-851
         return r
     x, px, y, py, z, d = r
     dp1 = beti + d
-    c, s = math.cos(theta), math.sin(theta)
+    c, s = fm.cos(theta), fm.sin(theta)
     pz = pxyz(dp1, px, py)
     d2 = pxyz(dp1, 0.0, py)
     pxn = px * c + (pz - h * x) * s
-    das = math.asin(jclamp(px / d2)) - math.asin(jclamp(pxn / d2))
-    num = x * (px * math.sin(2.0 * theta) + s * s * (2.0 * pz - h * x))
+    das = fm.asin(jclamp(px / d2)) - fm.asin(jclamp(pxn / d2))
+    num = x * (px * fm.sin(2.0 * theta) + s * s * (2.0 * pz - h * x))
     den = pxyz(dp1, pxn, py) + pz * c - px * s
     return (x * c + num / den, pxn, y + py * (theta / h + das / h), py, z + dp1 / h * (theta + das), d)
 
@@ -354,10 +359,10 @@ def body(r, h, L, beti):  # exact_bend_body, tracking.jl:858-894
         nl = L / pz
         return (x + px * nl, px, y + py * nl, py, z + nl * dp1 - L * beti, d)
     pzmx = pz - (1.0 + x * h)
-    cs, sn = math.cos(h * L), math.sin(h * L)
+    cs, sn = fm.cos(h * L), fm.sin(h * L)
     pxn = px * cs + pzmx * sn
     d2 = pxyz(dp1, 0.0, py)
-    das = L + (math.asin(jclamp(px / d2)) - math.asin(jclamp(pxn / d2))) / h
+    das = L + (fm.asin(jclamp(px / d2)) - fm.asin(jclamp(pxn / d2))) / h
     xn = (pxyz(dp1, pxn, py) - pzmx * cs + px * sn - 1.0) / h
     return (xn, pxn, y + py * das, py, z + dp1 * das - L * beti, d)
 
@@ -426,7 +431,7 @@ def apply_pass(e, r, beti):
         if e["energy"] > 0.0:
             nv = e["volt"] / e["energy"]
             ph = TWO_PI * e["freq"] * ((r[4] - e["lag"]) / C_LIGHT) - e["philag"]
-            r = r[:5] + (r[5] - nv * math.sin(ph) / (beta * beta),)
+            r = r[:5] + (r[5] - nv * fm.sin(ph) / (beta * beta),)
         if e["L"] > 0.0:
             r = drift(r, e["L"] / 2.0, beti)
         return r
@@ -438,7 +443,7 @@ def apply_pass(e, r, beti):
         pn = 1.0 / (1.0 + d)
         xpr, ypr = px * pn, py * pn
         H = ks * pn / 2.0
-        S, C = math.sin(L * H), math.cos(L * H)
+        S, C = fm.sin(L * H), fm.cos(L * H)
         xn = x * C * C + xpr * C * S / H + y * C * S + ypr * S * S / H
         pxn = (-x * H * C * S + xpr * C * C - y * H * S * S + ypr * C * S) / pn
         yn = -x * C * S - xpr * S * S / H + y * C * C + ypr * C * S / H
@@ -465,7 +470,7 @@ def apply_pass(e, r, beti):
         if ang == 0.0:
             return r
         x, px, y, py, z, d = r
-        ca, sa, ta = math.cos(ang), math.sin(ang), math.tan(ang)
+        ca, sa, ta = fm.cos(ang), fm.sin(ang), fm.tan(ang)
         pz2 = 1.0 + 2.0 * d * beti + d * d - px * px - py * py
         if pz2 <= 0.0:
             return nan6()
@@ -483,8 +488,8 @@ def apply_pass(e, r, beti):
         ang = k * r[4] + phi
         if e["L"] > 0.0:
             r = drift(r, e["L"] / 2.0, beti)
-        pxn = r[1] + (volt / E) * math.sin(ang * beti)
-        dn = r[5] - (k * volt / E * beti) * r[0] * math.cos(ang * beti)
+        pxn = r[1] + (volt / E) * fm.sin(ang * beti)
+        dn = r[5] - (k * volt / E * beti) * r[0] * fm.cos(ang * beti)
         r = (r[0], pxn, r[2], r[3], r[4], dn)
         if e["L"] > 0.0:
             r = drift(r, e["L"] / 2.0, beti)
@@ -496,7 +501,7 @@ def apply_pass(e, r, beti):
             return r
         E = max(abs(e["energy"]), EPS)
         k, phis = e["param"][0], e["param"][1]
-        sv = math.sin(k * r[4] + phis) - math.sin(phis)
+        sv = fm.sin(k * r[4] + phis) - fm.sin(phis)
         return r[:5] + (r[5] + (e["volt"] / (b2 * E)) * sv,)
     if kind == "LONGITUDINAL_RF_MAP":  # tracking.jl:1575-1585
         alphac, k, h = e["param"][0], e["param"][1], e["param"][2]

@@ -1,0 +1,63 @@
+"""The shared transcendental functions (tp_libm.h, used by the kernels and the
+oracle) against the C library: within 1 ulp over the ranges the maps use and
+far beyond them."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle_ref
+
+FUNCS = {"asin": 0, "sin": 1, "cos": 2, "tan": 3, "atan": 4}
+
+
+def ulp_diff(a, b):
+    ia = a.view(np.int64)
+    ib = b.view(np.int64)
+    ia = np.where(ia < 0, np.int64(-0x8000000000000000) - ia, ia)
+    ib = np.where(ib < 0, np.int64(-0x8000000000000000) - ib, ib)
+    return np.abs(ia - ib)
+
+
+def run(name, x):
+    lib = oracle_ref.lib()
+    lib.orc_libm.argtypes = [C.c_int32, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    ours = np.empty_like(x)
+    clib = np.empty_like(x)
+    lib.orc_libm(FUNCS[name], x.ctypes.data_as(C.c_void_p), len(x), ours.ctypes.data_as(C.c_void_p),
+                 clib.ctypes.data_as(C.c_void_p))
+    return ours, clib
+
+
+def samples(lo, hi, n, rng, log=False):
+    if log:
+        v = np.exp(rng.uniform(np.log(lo), np.log(hi), n))
+        return v * rng.choice([-1.0, 1.0], n)
+    return rng.uniform(lo, hi, n)
+
+
+@pytest.mark.parametrize("name,ranges", [
+    ("asin", [(-1.0, 1.0, False), (1e-12, 0.5, True), (0.5, 1.0, False), (0.97, 1.0, False)]),
+    ("sin", [(-np.pi / 4, np.pi / 4, False), (1e-12, 1.0, True), (-50.0, 50.0, False), (1.0, 1e5, True)]),
+    ("cos", [(-np.pi / 4, np.pi / 4, False), (1e-12, 1.0, True), (-50.0, 50.0, False), (1.0, 1e5, True)]),
+    ("tan", [(-np.pi / 4, np.pi / 4, False), (1e-12, 1.0, True), (-1.5, 1.5, False), (1.0, 1e5, True)]),
+    ("atan", [(-3.0, 3.0, False), (1e-12, 1e12, True), (0.4, 2.5, False)]),
+])
+def test_within_one_ulp_of_c_library(name, ranges):
+    rng = np.random.Generator(np.random.Philox(7))
+    for lo, hi, log in ranges:
+        x = samples(lo, hi, 200000, rng, log)
+        ours, clib = run(name, x)
+        d = ulp_diff(ours, clib)
+        assert d.max() <= 1, f"{name} on [{lo}, {hi}]: {d.max()} ulp"
+        assert (d == 0).mean() > 0.8, f"{name}: too many 1-ulp differences"
+
+
+def test_special_values():
+    for name in FUNCS:
+        ours, clib = run(name, np.array([0.0, -0.0, np.nan, np.inf, -np.inf, 1.0, -1.0, 1e-300]))
+        same = (ours == clib) | (np.isnan(ours) & np.isnan(clib))
+        if name == "asin":
+            same[3:5] = np.isnan(ours[3:5])
+        assert same.all(), (name, ours, clib)

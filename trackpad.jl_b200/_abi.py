@@ -61,7 +61,7 @@ class TpMisalign(C.Structure):
 class TpOpts(C.Structure):
     _fields_ = [
         ("size", C.c_int32), ("exact_hamiltonian", C.c_int32), ("device_pointers", C.c_int32),
-        ("fp_strict", C.c_int32), ("block_size", C.c_int32), ("ppt", C.c_int32), ("schedule", C.c_int32),
+        ("fp_contract", C.c_int32), ("block_size", C.c_int32), ("ppt", C.c_int32), ("schedule", C.c_int32),
         ("reserved0", C.c_int32), ("aperture_x", C.c_double), ("aperture_y", C.c_double), ("stream", C.c_void_p),
     ]
 
@@ -71,7 +71,7 @@ class TpStats(C.Structure):
         ("particles", C.c_int64), ("survivors", C.c_int64), ("element_passes", C.c_int64), ("units", C.c_double),
         ("flops", C.c_double), ("kernel_ms", C.c_double), ("total_ms", C.c_double), ("h2d_bytes", C.c_int64),
         ("d2h_bytes", C.c_int64), ("block_size", C.c_int32), ("ppt", C.c_int32), ("grid", C.c_int32),
-        ("launches", C.c_int32), ("schedule", C.c_int32), ("fp_strict", C.c_int32),
+        ("launches", C.c_int32), ("schedule", C.c_int32), ("fp_contract", C.c_int32),
     ]
 
 

@@ -2,14 +2,16 @@
 // the device element program (tp_program.h), plus the algorithmic FLOP model.
 //
 // Host constants are computed with the operations, operands and order the
-// reference uses per particle (built with -ffp-contract=off), so hoisting them
-// out of the particle loop does not change a single bit of the result.
+// reference uses per particle (built with -ffp-contract=off, transcendental
+// functions from tp_libm.h), so hoisting them out of the particle loop does not
+// change a single bit of the result.
 #include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "tp_internal.h"
+#include "tp_libm.h"
 
 namespace tp {
 
@@ -64,8 +66,8 @@ void yoshida_consts(double L, int n, double* L1, double* L2, double* K1, double*
 // kick_angle folding (src/tracking.jl:396-411, 668-682, 931-940).
 void fold_kick(const tp_elem& e, double* pa, double* pb) {
     if (e.L > 0.0) {
-        pb[0] = pb[0] - std::sin(e.kick_angle[0]) / e.L;
-        pa[0] = pa[0] + std::sin(e.kick_angle[1]) / e.L;
+        pb[0] = pb[0] - libm::sin(e.kick_angle[0]) / e.L;
+        pa[0] = pa[0] + libm::sin(e.kick_angle[1]) / e.L;
     }
 }
 
@@ -166,10 +168,10 @@ static Rec compile_rec(const tp_elem& e) {
                 if (fint == 0.0 || e.gap == 0.0 || method == 0) {
                     corr = 0.0;
                 } else {
-                    double sedge = std::sin(ang), cedge = std::cos(ang);
+                    double sedge = libm::sin(ang), cedge = libm::cos(ang);
                     corr = irho * e.gap * fint * (1.0 + sedge * sedge) / cedge;
                 }
-                *fx = irho * std::tan(ang);
+                *fx = irho * libm::tan(ang);
                 *eang = ang;
                 *fc = corr;
             };
@@ -197,27 +199,27 @@ static Rec compile_rec(const tp_elem& e) {
             r.w[eb::GK] = e.gk;
             if (e.e1 != 0.0) {
                 r.h.flags |= RF_YROT_IN;
-                r.w[eb::YC_IN] = std::cos(e.e1);
-                r.w[eb::YS_IN] = std::sin(e.e1);
+                r.w[eb::YC_IN] = libm::cos(e.e1);
+                r.w[eb::YS_IN] = libm::sin(e.e1);
             }
             if (e.e2 != 0.0) {
                 r.h.flags |= RF_YROT_OUT;
-                r.w[eb::YC_OUT] = std::cos(e.e2);
-                r.w[eb::YS_OUT] = std::sin(e.e2);
+                r.w[eb::YC_OUT] = libm::cos(e.e2);
+                r.w[eb::YS_OUT] = libm::sin(e.e2);
             }
             if (e.fringe_bend_entrance != 0) r.h.flags |= RF_FRINGE_IN;
             if (e.fringe_bend_exit != 0) r.h.flags |= RF_FRINGE_OUT;
             if (!(std::fabs(irho) < 1e-6)) {
                 r.h.flags |= RF_EDGE;  // bend_edge returns r unchanged when |rhoinv| < 1e-6
                 double t_in = -e.e1, t_out = -e.e2;
-                r.w[eb::EC_IN] = std::cos(t_in);
-                r.w[eb::ES_IN] = std::sin(t_in);
-                r.w[eb::ES2_IN] = std::sin(2.0 * t_in);
+                r.w[eb::EC_IN] = libm::cos(t_in);
+                r.w[eb::ES_IN] = libm::sin(t_in);
+                r.w[eb::ES2_IN] = libm::sin(2.0 * t_in);
                 r.w[eb::ETH_IN] = t_in;
                 r.w[eb::ETHH_IN] = t_in / irho;
-                r.w[eb::EC_OUT] = std::cos(t_out);
-                r.w[eb::ES_OUT] = std::sin(t_out);
-                r.w[eb::ES2_OUT] = std::sin(2.0 * t_out);
+                r.w[eb::EC_OUT] = libm::cos(t_out);
+                r.w[eb::ES_OUT] = libm::sin(t_out);
+                r.w[eb::ES2_OUT] = libm::sin(2.0 * t_out);
                 r.w[eb::ETH_OUT] = t_out;
                 r.w[eb::ETHH_OUT] = t_out / irho;
             } else {
@@ -226,17 +228,17 @@ static Rec compile_rec(const tp_elem& e) {
             if (e.num_int_steps == 0) {
                 r.h.flags |= RF_BODY_ONE;
                 r.w[eb::L1] = e.L;
-                r.w[eb::CS1] = std::cos(irho * e.L);
-                r.w[eb::SN1] = std::sin(irho * e.L);
+                r.w[eb::CS1] = libm::cos(irho * e.L);
+                r.w[eb::SN1] = libm::sin(irho * e.L);
             } else {
                 double pa[4], pb[4];
                 for (int i = 0; i < 4; ++i) { pa[i] = e.polynom_a[i]; pb[i] = e.polynom_b[i]; }
                 fold_kick(e, pa, pb);
                 yoshida_consts(e.L, e.num_int_steps, &r.w[eb::L1], &r.w[eb::L2], &r.w[eb::K1], &r.w[eb::K2]);
-                r.w[eb::CS1] = std::cos(irho * r.w[eb::L1]);
-                r.w[eb::SN1] = std::sin(irho * r.w[eb::L1]);
-                r.w[eb::CS2] = std::cos(irho * r.w[eb::L2]);
-                r.w[eb::SN2] = std::sin(irho * r.w[eb::L2]);
+                r.w[eb::CS1] = libm::cos(irho * r.w[eb::L1]);
+                r.w[eb::SN1] = libm::sin(irho * r.w[eb::L1]);
+                r.w[eb::CS2] = libm::cos(irho * r.w[eb::L2]);
+                r.w[eb::SN2] = libm::sin(irho * r.w[eb::L2]);
                 for (int i = 0; i < 4; ++i) { r.w[eb::PA + i] = pa[i]; r.w[eb::PB + i] = pb[i]; }
                 // With max_order 0 the kick is px -= K*pb[0], py += K*pa[0]: exact no-ops
                 // when both coefficients are zero (only the sign of a zero can change).
@@ -281,9 +283,9 @@ static Rec compile_rec(const tp_elem& e) {
             double angle = -e.angle;
             if (angle == 0.0) { r.h.kind = DK_IDENTITY; break; }
             r.h.kind = DK_YROTATION;
-            r.w[yr::CA] = std::cos(angle);
-            r.w[yr::SA] = std::sin(angle);
-            r.w[yr::TA] = std::tan(angle);
+            r.w[yr::CA] = libm::cos(angle);
+            r.w[yr::SA] = libm::sin(angle);
+            r.w[yr::TA] = libm::tan(angle);
             r.nw = yr::WORDS;
             break;
         }
@@ -302,7 +304,7 @@ static Rec compile_rec(const tp_elem& e) {
             r.w[acc::E] = jmax_eps(std::fabs(e.energy));
             r.w[acc::K] = e.param[0];
             r.w[acc::PHIS] = e.param[1];
-            r.w[acc::SINPHIS] = std::sin(e.param[1]);
+            r.w[acc::SINPHIS] = libm::sin(e.param[1]);
             r.nw = acc::WORDS;
             break;
         case TP_LONGITUDINAL_RF_MAP:  // tracking.jl:1575-1585

@@ -10,11 +10,13 @@
 //   bd  = beti + delta                 (drift6 z update; dp1 of the exact bend)
 //   opd = 1 + delta
 // Multiplication of those cached values reproduces the reference's per-call
-// values exactly, because IEEE operations are deterministic.
+// values exactly, because IEEE operations are deterministic.  sin, cos, tan,
+// asin and atan come from tp_libm.h (the same bits on host and device).
 #pragma once
 #include <math_constants.h>
 #include <stdint.h>
 
+#include "tp_libm.h"
 #include "tp_program.h"
 
 namespace tp {
@@ -133,13 +135,13 @@ __device__ __forceinline__ void edge_fringe(P6& s, double irho, double fx, doubl
     double fy;
     if (method == 3) {
         double q = s.px / opd;
-        fy = irho * tan(is_exit ? (e - fc - q) : (e - fc + q));
+        fy = irho * libm::tan(is_exit ? (e - fc - q) : (e - fc + q));
     } else if (method == 2) {
         if (fc_zero) fy = zero_quotient_ok(opd) ? fx / opd : CUDART_NAN;
-        else fy = irho * tan(e - fc / opd) / opd;
+        else fy = irho * libm::tan(e - fc / opd) / opd;
     } else {
         if (fc_zero) fy = zero_quotient_ok(opd) ? fx : CUDART_NAN;
-        else fy = irho * tan(e - fc / opd);
+        else fy = irho * libm::tan(e - fc / opd);
     }
     s.px = s.px + s.x * fx;
     s.py = s.py - s.y * fy;
@@ -205,14 +207,14 @@ static __device__ __noinline__ void bend_fringe(P6& r, double irho, double gK, d
     double yp = py / pz;
     double term1 = 1.0 + xp * xp * (2.0 + yp * yp);
     double term2 = xp / (1.0 + yp * yp);
-    double phi = -b0 * tan(b0 * gK * term1 * pz - atan(term2));
+    double phi = -b0 * libm::tan(b0 * gK * term1 * pz - libm::atan(term2));
     double px2 = px * px;
     double py2 = py * py;
     double pz2 = pz * pz;
     double pz4 = pz2 * pz2;
     double py2z2 = (py2 + pz2);
-    double arg_sec = (b0 * gK * (pz4 + px2 * (py2 + 2.0 * pz2))) / (pz2 * pz) - atan(px * pz / (py2 + pz2));
-    double sec = 1.0 / cos(arg_sec);
+    double arg_sec = (b0 * gK * (pz4 + px2 * (py2 + 2.0 * pz2))) / (pz2 * pz) - libm::atan(px * pz / (py2 + pz2));
+    double sec = 1.0 / libm::cos(arg_sec);
     double powsec = sec * sec;
     double py4 = py2 * py2;
     double py6 = py4 * py2;
@@ -259,7 +261,7 @@ static __device__ __noinline__ void bend_edge(P6& r, double rhoinv, double c, do
     double px_new = r.px * c + (pz - rhoinv * r.x) * s;
     double val1 = jclamp(r.px / d2);
     double val2 = jclamp(px_new / d2);
-    double dasin = asin(val1) - asin(val2);
+    double dasin = libm::asin(val1) - libm::asin(val2);
     double num = r.x * (r.px * s2 + s * s * (2.0 * pz - rhoinv * r.x));
     double den = pxyz(dp1sq, px_new, r.py) + pz * c - r.px * s;
     double x_new = r.x * c + num / den;
@@ -285,7 +287,7 @@ __device__ __forceinline__ void body_one(P6& r, double irho, double L, double Lb
     double d2 = pxyz(dp1sq, 0.0, r.py);
     double val1 = jclamp(r.px / d2);
     double val2 = jclamp(px_new / d2);
-    double dasin = L + (asin(val1) - asin(val2)) / irho;
+    double dasin = L + (libm::asin(val1) - libm::asin(val2)) / irho;
     double x_new = (pxyz(dp1sq, px_new, r.py) - pzmx * cs + r.px * sn - 1.0) / irho;
     r.y = r.y + r.py * dasin;
     r.z = r.z + dp1 * dasin - Lbeti;
@@ -309,14 +311,14 @@ __device__ __forceinline__ void body_carry_init(const P6& r, double dp1, BodyCar
     b.d2 = v0 > 0.0 ? sqrt(v0) : 0.0;
     double v = b.dp1sq - r.px * r.px - b.pysq;
     b.pz = v > 0.0 ? sqrt(v) : 0.0;
-    b.as1 = asin(jclamp(r.px / b.d2));
+    b.as1 = libm::asin(jclamp(r.px / b.d2));
 }
 
 __device__ __forceinline__ void body_carry_step(P6& r, BodyCarry& b, double irho, double L, double Lbeti, double cs,
                                                 double sn, double dp1) {
     double pzmx = b.pz - (1.0 + r.x * irho);
     double px_new = r.px * cs + pzmx * sn;
-    double as2 = asin(jclamp(px_new / b.d2));
+    double as2 = libm::asin(jclamp(px_new / b.d2));
     double dasin = L + (b.as1 - as2) / irho;
     double v = b.dp1sq - px_new * px_new - b.pysq;
     double pz_new = v > 0.0 ? sqrt(v) : 0.0;
@@ -400,7 +402,7 @@ __device__ __forceinline__ void rf_cavity(P6& s, const double* w, const RecHdr& 
     }
     if (h.flags & RF_ENERGY) {
         double phase = w[rf::W] * ((s.z - w[rf::LAG]) / C_LIGHT) - w[rf::PHILAG];
-        s.d = s.d - w[rf::NV] * sin(phase) / beta2;
+        s.d = s.d - w[rf::NV] * libm::sin(phase) / beta2;
     }
     if (h.flags & RF_LPOS) {
         DCache c;
@@ -423,8 +425,8 @@ __device__ __noinline__ void solenoid(P6& s, const double* w, double beti) {
     double p_norm = 1.0 / (1.0 + s.d);
     double x = s.x, xpr = s.px * p_norm, y = s.y, ypr = s.py * p_norm;
     double H = ks * p_norm / 2.0;
-    double S = sin(L * H);
-    double C = cos(L * H);
+    double S = libm::sin(L * H);
+    double C = libm::cos(L * H);
     double x_new = x * C * C + xpr * C * S / H + y * C * S + ypr * S * S / H;
     double px_new = (-x * H * C * S + xpr * C * C - y * H * S * S + ypr * C * S) / p_norm;
     double y_new = -x * C * S - xpr * S * S / H + y * C * C + ypr * C * S / H;
@@ -483,8 +485,8 @@ __device__ __forceinline__ void crab_cavity(P6& s, const double* w, const RecHdr
         make_cache(s, beti, c);
         drift<EXACT>(s, w[crab::LH], w[crab::LH] * beti, c);
     }
-    double px_new = s.px + (volt / E) * sin(ang * beti);
-    double delta_new = s.d - (k * volt / E * beti) * s.x * cos(ang * beti);
+    double px_new = s.px + (volt / E) * libm::sin(ang * beti);
+    double delta_new = s.d - (k * volt / E * beti) * s.x * libm::cos(ang * beti);
     s.px = px_new;
     s.d = delta_new;
     if (h.flags & RF_LPOS) {
@@ -497,7 +499,7 @@ __device__ __forceinline__ void crab_cavity(P6& s, const double* w, const RecHdr
 // pass!(::AccelCavity) (src/tracking.jl:1549-1559).
 __device__ __forceinline__ void accel_cavity(P6& s, const double* w, double beta2) {
     if (beta2 <= EPSD) return;
-    double sv = sin(w[acc::K] * s.z + w[acc::PHIS]) - w[acc::SINPHIS];
+    double sv = libm::sin(w[acc::K] * s.z + w[acc::PHIS]) - w[acc::SINPHIS];
     s.d = s.d + (w[acc::VOLT] / (beta2 * w[acc::E])) * sv;
 }
 

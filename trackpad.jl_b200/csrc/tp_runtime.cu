@@ -83,6 +83,9 @@ struct tp_batch {
     double* beti_v = nullptr;
     int64_t* poff = nullptr;
     MisalignDev* mis = nullptr;
+    double* prefix = nullptr;          // per-variant inclusive flop prefix sums: exact drift, then linearised
+    int64_t* prefix_off = nullptr;     // offsets of each variant's prefix (nvar + 1)
+    int64_t prefix_words = 0;          // length of one prefix set
     std::vector<int64_t> h_toff;
     std::vector<int32_t> h_nelem;
     std::vector<int64_t> h_mis_off;    // misalignment row offset per variant
@@ -239,6 +242,19 @@ int upload_lattice(tp_ctx* c, tp_lattice* L) {
         TP_CUDA(cudaMalloc(&d.mis, md.size() * sizeof(MisalignDev)));
         TP_CUDA(cudaMemcpy(d.mis, md.data(), md.size() * sizeof(MisalignDev), cudaMemcpyHostToDevice));
     }
+    {   // inclusive flop prefix sums: exact-drift set, then linearised set
+        const size_t n = std::max<size_t>(L->elems.size(), 1);
+        std::vector<double> pre(2 * n, 0.0);
+        double ae = 0.0, al = 0.0;
+        for (size_t i = 0; i < L->elems.size(); ++i) {
+            ae += L->flops_exact[i];
+            al += L->flops_lin[i];
+            pre[i] = ae;
+            pre[n + i] = al;
+        }
+        TP_CUDA(cudaMalloc(&d.prefix, pre.size() * sizeof(double)));
+        TP_CUDA(cudaMemcpy(d.prefix, pre.data(), pre.size() * sizeof(double), cudaMemcpyHostToDevice));
+    }
     if (L->has_sched && !L->sched_table.empty()) {
         d.sched_bytes = L->sched_table.size() * sizeof(double);
         TP_CUDA(cudaMalloc(&d.sched, d.sched_bytes));
@@ -248,17 +264,8 @@ int upload_lattice(tp_ctx* c, tp_lattice* L) {
     return TP_OK;
 }
 
-int upload_prefix(tp_ctx* c, tp_lattice* L, bool exact, double** out) {
-    std::vector<double> pre(std::max<size_t>(L->elems.size(), 1), 0.0);
-    const std::vector<double>& f = exact ? L->flops_exact : L->flops_lin;
-    double acc = 0.0;
-    for (size_t i = 0; i < L->elems.size(); ++i) { acc += f[i]; pre[i] = acc; }
-    DevLattice& d = L->dev[c->device];
-    if (!d.prefix) TP_CUDA(cudaMalloc(&d.prefix, pre.size() * sizeof(double)));
-    TP_CUDA(cudaMemcpyAsync(d.prefix, pre.data(), pre.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    TP_CUDA(cudaStreamSynchronize(c->stream));
-    *out = d.prefix;
-    return TP_OK;
+double* prefix_of(tp_ctx* c, tp_lattice* L, bool exact) {
+    return L->dev[c->device].prefix + (exact ? 0 : std::max<size_t>(L->elems.size(), 1));
 }
 
 tp_opts default_opts(const tp_opts* o) {
@@ -556,9 +563,7 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
         if (!d_lt) d_lt = c->lost_turn;
         if (!d_le) d_le = c->lost_elem;
     }
-    double* prefix = nullptr;
-    st = upload_prefix(c, L, exact, &prefix);
-    if (st != TP_OK) return st;
+    double* prefix = prefix_of(c, L, exact);
     DevLattice& dl = L->dev[c->device];
 
     TrackArgs a{};
@@ -594,7 +599,7 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     a.refill = schedule == 2 ? 1 : 0;
     int block = o.block_size > 0 ? o.block_size : 128;
     block = std::max(32, std::min(256, block / 32 * 32));
-    const bool strict = o.fp_strict != 0;
+    const bool strict = o.fp_contract == 0;
     int bps = 0;
     int oerr = strict ? occupancy_track_strict(block, 1, smem, &bps) : occupancy_track_fast(block, 1, smem, &bps);
     if (oerr != 0 || bps <= 0) bps = 1;
@@ -648,7 +653,7 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     S.grid = grid;
     S.launches = 3 + (lost_turn ? 0 : 1) + (lost_elem ? 0 : 1);
     S.schedule = schedule;
-    S.fp_strict = strict ? 1 : 0;
+    S.fp_contract = strict ? 0 : 1;
     return TP_OK;
 }
 
@@ -713,6 +718,24 @@ TP_API int tp_batch_create(tp_ctx* c, const tp_lattice* const* lats, int32_t nva
     }
     b->h_toff[size_t(nvar)] = int64_t(table.size());
     b->table_words = table.size();
+    // FLOP prefix tables of every variant (exact drift set, then linearised set).
+    std::vector<double> pre_e, pre_l;
+    std::vector<int64_t> pre_off(size_t(nvar) + 1, 0);
+    for (int32_t v = 0; v < nvar; ++v) {
+        const tp_lattice* L = lats[v];
+        pre_off[size_t(v)] = int64_t(pre_e.size());
+        double ae = 0.0, al = 0.0;
+        for (size_t i = 0; i < L->elems.size(); ++i) {
+            ae += L->flops_exact[i];
+            al += L->flops_lin[i];
+            pre_e.push_back(ae);
+            pre_l.push_back(al);
+        }
+        if (L->elems.empty()) { pre_e.push_back(0.0); pre_l.push_back(0.0); }
+    }
+    pre_off[size_t(nvar)] = int64_t(pre_e.size());
+    b->prefix_words = int64_t(pre_e.size());
+    pre_e.insert(pre_e.end(), pre_l.begin(), pre_l.end());
     cudaError_t e = cudaMalloc(&b->table, std::max<size_t>(table.size(), 2) * sizeof(double));
     if (e == cudaSuccess) e = cudaMemcpy(b->table, table.data(), table.size() * sizeof(double), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&b->toff, 2 * (size_t(nvar) + 1) * sizeof(int64_t));
@@ -721,6 +744,11 @@ TP_API int tp_batch_create(tp_ctx* c, const tp_lattice* const* lats, int32_t nva
     if (e == cudaSuccess) e = cudaMemcpy(b->nelem_v, b->h_nelem.data(), size_t(nvar) * sizeof(int32_t), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&b->beti_v, size_t(nvar) * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&b->poff, (size_t(nvar) + 1) * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&b->prefix, pre_e.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpy(b->prefix, pre_e.data(), pre_e.size() * sizeof(double), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&b->prefix_off, pre_off.size() * sizeof(int64_t));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->prefix_off, pre_off.data(), pre_off.size() * sizeof(int64_t), cudaMemcpyHostToDevice);
     if (e == cudaSuccess && !mis.empty()) {
         e = cudaMalloc(&b->mis, mis.size() * sizeof(MisalignDev));
         if (e == cudaSuccess) e = cudaMemcpy(b->mis, mis.data(), mis.size() * sizeof(MisalignDev), cudaMemcpyHostToDevice);
@@ -742,6 +770,8 @@ TP_API int tp_batch_destroy(tp_batch* b) {
     if (b->graph) cudaGraphExecDestroy(b->graph);
     cudaFree(b->table); cudaFree(b->toff); cudaFree(b->nelem_v); cudaFree(b->beti_v); cudaFree(b->poff);
     cudaFree(b->mis);
+    cudaFree(b->prefix);
+    cudaFree(b->prefix_off);
     cudaSetDevice(cur);
     cudaGetLastError();
     delete b;
@@ -773,7 +803,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     cudaStream_t s = o.stream ? static_cast<cudaStream_t>(o.stream) : c->stream;
     const bool dev = o.device_pointers != 0;
     const bool exact = o.exact_hamiltonian != 0;
-    const bool strict = o.fp_strict != 0;
+    const bool strict = o.fp_contract == 0;
     int st = ensure_capacity(c, n);
     if (st != TP_OK) return st;
     double* d_coords = dev ? coords : c->coords;
@@ -800,25 +830,8 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     TP_CUDA(cudaMemcpyAsync(b->toff, offs.data(), offs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s));
     TP_CUDA(cudaMemcpyAsync(b->beti_v, beti, size_t(nvar) * sizeof(double), cudaMemcpyHostToDevice, s));
     TP_CUDA(cudaMemcpyAsync(b->poff, poff, (size_t(nvar) + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
-    std::vector<double> pre;
-    std::vector<int64_t> pre_off(size_t(nvar) + 1, 0);
-    for (int32_t v = 0; v < nvar; ++v) {
-        const tp_lattice* L = b->lats[size_t(v)];
-        pre_off[size_t(v)] = int64_t(pre.size());
-        double acc = 0.0;
-        for (size_t i = 0; i < L->elems.size(); ++i) {
-            acc += exact ? L->flops_exact[i] : L->flops_lin[i];
-            pre.push_back(acc);
-        }
-        if (L->elems.empty()) pre.push_back(0.0);
-    }
-    pre_off[size_t(nvar)] = int64_t(pre.size());
-    double* d_pre = nullptr;
-    int64_t* d_pre_off = nullptr;
-    TP_CUDA(cudaMallocAsync(&d_pre, pre.size() * sizeof(double), s));
-    TP_CUDA(cudaMallocAsync(&d_pre_off, pre_off.size() * sizeof(int64_t), s));
-    TP_CUDA(cudaMemcpyAsync(d_pre, pre.data(), pre.size() * sizeof(double), cudaMemcpyHostToDevice, s));
-    TP_CUDA(cudaMemcpyAsync(d_pre_off, pre_off.data(), pre_off.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    const double* d_pre = b->prefix + (exact ? 0 : b->prefix_words);
+    const int64_t* d_pre_off = b->prefix_off;
 
     TrackArgs a{};
     a.table = b->table;
@@ -851,7 +864,10 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     grid = std::max(grid, 1);
     int sg = grid_for(n, 256, c->sm_count);
 
-    auto enqueue = [&](cudaStream_t q) -> int {
+    // `timed`: record the kernel events inside the sequence (not during graph
+    // capture: a captured event record does not time; the graph launch is
+    // bracketed by the events instead).
+    auto enqueue = [&](cudaStream_t q, bool timed) -> int {
         TP_CUDA(cudaMemsetAsync(c->counters, 0, 8 * sizeof(unsigned long long), q));
         TP_CUDA(cudaMemsetAsync(c->err, 0, 4 * sizeof(int32_t), q));
         TP_CUDA(cudaMemsetAsync(c->flops_acc, 0, 2 * sizeof(double), q));
@@ -859,10 +875,10 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
         if (!(dev && lost_elem)) k_fill_i32<<<sg, 256, 0, q>>>(d_le, n, -1);
         k_alive_mask<<<sg, 256, 0, q>>>(d_lost, n, c->alive0, c->counters + 2);
         TP_CUDA(cudaGetLastError());
-        TP_CUDA(cudaEventRecord(c->ev0, q));
+        if (timed) TP_CUDA(cudaEventRecord(c->ev0, q));
         int le = strict ? launch_track_strict(a, grid, block, 1, 0, q) : launch_track_fast(a, grid, block, 1, 0, q);
         if (le != 0) return cuda_err(cudaError_t(le), "batched track kernel launch");
-        TP_CUDA(cudaEventRecord(c->ev1, q));
+        if (timed) TP_CUDA(cudaEventRecord(c->ev1, q));
         k_work_stats<<<sg, 256, 0, q>>>(c->alive0, d_lost, d_lt, d_le, n, d_pre, b->poff, d_pre_off, b->nelem_v, nvar,
                                         0, nturns, turn0, c->counters + 3, c->flops_acc);
         TP_CUDA(cudaGetLastError());
@@ -880,7 +896,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
             TP_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
             TP_CUDA(cudaStreamSynchronize(s));
             TP_CUDA(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-            int est = enqueue(cap);
+            int est = enqueue(cap, false);
             cudaGraph_t graph = nullptr;
             cudaError_t ce = cudaStreamEndCapture(cap, &graph);
             cudaStreamDestroy(cap);
@@ -893,9 +909,11 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
             b->g_limx = a.limx; b->g_limy = a.limy; b->g_coords = d_coords; b->g_lost = d_lost;
             b->g_poff.assign(poff, poff + nvar + 1);
         }
+        TP_CUDA(cudaEventRecord(c->ev0, s));
         TP_CUDA(cudaGraphLaunch(b->graph, s));
+        TP_CUDA(cudaEventRecord(c->ev1, s));
     } else {
-        st = enqueue(s);
+        st = enqueue(s, true);
         if (st != TP_OK) return st;
     }
     if (!dev) {
@@ -909,8 +927,6 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     double fl[2];
     TP_CUDA(cudaMemcpyAsync(cnt, c->counters, sizeof cnt, cudaMemcpyDeviceToHost, s));
     TP_CUDA(cudaMemcpyAsync(fl, c->flops_acc, sizeof fl, cudaMemcpyDeviceToHost, s));
-    TP_CUDA(cudaFreeAsync(d_pre, s));
-    TP_CUDA(cudaFreeAsync(d_pre_off, s));
     TP_CUDA(cudaStreamSynchronize(s));
     st = check_device_error(c);
     if (st != TP_OK) return st;
@@ -931,7 +947,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     S.grid = grid;
     S.launches = 3 + ((dev && lost_turn) ? 0 : 1) + ((dev && lost_elem) ? 0 : 1);
     S.schedule = 3;
-    S.fp_strict = strict ? 1 : 0;
+    S.fp_contract = strict ? 0 : 1;
     return TP_OK;
 }
 
@@ -944,7 +960,7 @@ TP_API int tp_probe_fp64_peak(tp_ctx* c, double* tflops_out) {
     TP_CUDA(cudaSetDevice(c->device));
     double* out = nullptr;
     TP_CUDA(cudaMalloc(&out, sizeof(double)));
-    const int block = 256, grid = c->sm_count * 8, iters = 1 << 14;
+    const int block = 256, grid = c->sm_count * 8, iters = 1 << 12;
     double best = 0.0;
     for (int rep = 0; rep < 4; ++rep) {
         TP_CUDA(cudaEventRecord(c->ev0, c->stream));

@@ -271,12 +271,12 @@ def spos(lat, time=0.0, turn=0):
 # ---------------------------------------------------------------------------
 # Tracking calls
 # ---------------------------------------------------------------------------
-def _opts(aperture, exact, strict, device, block_size=0, schedule=0, stream=None):
+def _opts(aperture, exact, contract, device, block_size=0, schedule=0, stream=None):
     o = _abi.TpOpts()
     o.size = C.sizeof(_abi.TpOpts)
     o.exact_hamiltonian = 1 if exact else 0
     o.device_pointers = 1 if device else 0
-    o.fp_strict = 1 if strict else 0
+    o.fp_contract = 1 if contract else 0
     o.block_size = int(block_size)
     o.schedule = int(schedule)
     if aperture is not None:
@@ -357,14 +357,15 @@ class _Buffers:
 
 
 def ringpass_(coords, lat, beam, lost_flags, nturns, *, time=0.0, dt_turn=0.0, turn=0, aperture=None,
-              lost_turn=None, lost_elem=None, exact=True, strict=False, block_size=0, schedule=0, stream=None):
+              lost_turn=None, lost_elem=None, exact=True, contract=False, block_size=0, schedule=0, stream=None):
     """ringpass!(coords, lat, beam, lost_flags, nturns; time, dt_turn, turn) on the GPU.
 
     Extra keywords: `aperture` (half width, or (ax, ay)) adds the rectangular
     aperture check beside check_lost; `lost_turn`/`lost_elem` (int32, length N)
     receive the turn and 0-based element of each loss; `exact=False` selects the
-    linearised drift (USE_EXACT_HAMILTONIAN = false); `strict=True` runs the
-    kernel built without FMA contraction.
+    linearised drift (USE_EXACT_HAMILTONIAN = false); `contract=True` runs the
+    kernel built with FMA contraction (faster; its rounding differs from the
+    reference's operation order).
     """
     if not isinstance(lat, Lattice):
         lat = Lattice(lat)
@@ -374,7 +375,7 @@ def ringpass_(coords, lat, beam, lost_flags, nturns, *, time=0.0, dt_turn=0.0, t
     b = _Buffers(coords, lost_flags, lost_turn, lost_elem)
     lat.set_schedule(time, dt_turn, turn, max(nturns, 1))
     dev = b.device_index if b.device else None
-    o = _opts(aperture, exact, strict, b.device, block_size, schedule, stream)
+    o = _opts(aperture, exact, contract, b.device, block_size, schedule, stream)
     st = _abi.lib().tp_ringpass(context(dev), lat.handle, b.coords, b.n, b.lost, b.lost_turn, b.lost_elem,
                                 C.c_double(beti(beam)), nturns, C.c_double(time), C.c_double(dt_turn), int(turn),
                                 C.byref(o))
@@ -390,7 +391,7 @@ def linepass_(coords, lat, beam, lost_flags, *, time=0.0, turn=0, **kw):
     b = _Buffers(coords, lost_flags, kw.pop("lost_turn", None), kw.pop("lost_elem", None))
     lat.set_schedule(time, 0.0, turn, 1)
     dev = b.device_index if b.device else None
-    o = _opts(kw.get("aperture"), kw.get("exact", True), kw.get("strict", False), b.device, kw.get("block_size", 0),
+    o = _opts(kw.get("aperture"), kw.get("exact", True), kw.get("contract", False), b.device, kw.get("block_size", 0),
               kw.get("schedule", 0), kw.get("stream"))
     st = _abi.lib().tp_linepass(context(dev), lat.handle, b.coords, b.n, b.lost, b.lost_turn, b.lost_elem,
                                 C.c_double(beti(beam)), C.c_double(time), int(turn), C.byref(o))
@@ -411,7 +412,7 @@ class Batch:
         self._handle = h
 
     def ringpass_(self, coords, poff, betis, lost_flags, nturns, *, turn=0, aperture=None, lost_turn=None,
-                  lost_elem=None, exact=True, strict=False, use_graph=True, block_size=0, stream=None):
+                  lost_elem=None, exact=True, contract=False, use_graph=True, block_size=0, stream=None):
         b = _Buffers(coords, lost_flags, lost_turn, lost_elem)
         poff = np.ascontiguousarray(poff, dtype=np.int64)
         betis = np.ascontiguousarray(betis, dtype=np.float64)
@@ -419,7 +420,7 @@ class Batch:
             raise ValueError("poff must have nvar+1 entries and betis nvar entries")
         if poff[-1] != b.n:
             raise ValueError("poff[-1] must equal the number of particles")
-        o = _opts(aperture, exact, strict, b.device, block_size, 0, stream)
+        o = _opts(aperture, exact, contract, b.device, block_size, 0, stream)
         st = _abi.lib().tp_ringpass_batched(context(self.device), self._handle, b.coords,
                                             poff.ctypes.data_as(C.c_void_p), b.lost, b.lost_turn, b.lost_elem,
                                             betis.ctypes.data_as(C.c_void_p), int(nturns), C.c_double(0.0),

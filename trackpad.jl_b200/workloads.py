@@ -21,13 +21,15 @@ SIGMA = (1e-4, 1e-5, 1e-4, 1e-5, 1e-3, 1e-4)  # x, px, y, py, z, delta
 # DBA strengths: k1 of the three quadrupole families and k2 of the two
 # sextupole families.  Drawn by oracle/search_dba.py (Philox seed 0, k1 from
 # +-U[0.5, 2.5] m^-2, k2 from +-U[20, 60] m^-3) as the first draw whose linear
-# cell map is stable in both planes with |trace/2| <= 0.9.
+# cell map is stable with |trace/2| <= 0.9, whose cell tunes (0.309, 0.396) keep
+# 0.04 away from the third- and fourth-order resonances the sextupoles of every
+# cell drive, and on which a 256-particle Gaussian beam survives 300 turns.
 DBA_FAMILIES = {
-    "Q1": 1.2821827924848423,
-    "Q2": -0.8465662929760225,
-    "Q3": 1.0737910720404733,
-    "S1": 35.585397914110914,
-    "S2": -28.31525487748862,
+    "Q1": 1.3067877421264442,
+    "Q2": -0.8455488336578774,
+    "Q3": 1.0102025344289203,
+    "S1": 38.679376805147385,
+    "S2": -29.5033306060304,
 }
 DBA_CELL = ["D", "Q1", "D", "Q2", "D", "B", "S1", "Q3", "S2", "D", "D", "S2", "Q3", "S1", "B", "D", "Q2", "D", "Q1", "D"]
 DBA_CELL_LENGTH = 25.0
