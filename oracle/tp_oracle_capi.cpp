@@ -132,6 +132,21 @@ double orc_beam_beti(double energy, double mass) { return beam_beti(energy, mass
 
 int orc_max_threads(void) { return omp_get_max_threads(); }
 
+// Markstein's reciprocal division q' = RN(q + r*y), q = RN(a*y), r = a - b*q,
+// y = RN(1/b), compared with IEEE a/b on n pairs: returns the number that differ.
+int64_t orc_check_rcp_div(const double* a, const double* b, int64_t n) {
+    int64_t bad = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        double y = 1.0 / b[i];
+        double q = a[i] * y;
+        double r = std::fma(-q, b[i], a[i]);
+        double q1 = std::fma(r, y, q);
+        double ref = a[i] / b[i];
+        if (!(q1 == ref || (std::isnan(q1) && std::isnan(ref)))) ++bad;
+    }
+    return bad;
+}
+
 // The shared transcendental functions (which: 0 asin, 1 sin, 2 cos, 3 tan,
 // 4 atan) and the C library's, on n arguments, for the accuracy tests.
 void orc_libm(int32_t which, const double* x, int64_t n, double* ours, double* clib) {

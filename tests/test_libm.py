@@ -61,3 +61,21 @@ def test_special_values():
         if name == "asin":
             same[3:5] = np.isnan(ours[3:5])
         assert same.all(), (name, ours, clib)
+
+
+@pytest.mark.parametrize("blo,bhi", [(0.5, 2.0), (1e-3, 1.0), (1.0, 1e3), (0.9, 1.1)])
+def test_reciprocal_division_is_exact(blo, bhi):
+    """The kernels divide by loop-invariant divisors (d2, irho) with Markstein's
+    sequence from RN(1/b); it must equal the IEEE quotient bit for bit."""
+    lib = oracle_ref.lib()
+    lib.orc_check_rcp_div.restype = C.c_int64
+    lib.orc_check_rcp_div.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+    rng = np.random.Generator(np.random.Philox(11))
+    n = 2_000_000
+    a = np.exp(rng.uniform(np.log(1e-20), np.log(1e3), n)) * rng.choice([-1.0, 1.0], n)
+    b = np.exp(rng.uniform(np.log(blo), np.log(bhi), n)) * rng.choice([-1.0, 1.0], n)
+    # include divisors with all-ones and all-zeros significands and random bit patterns
+    b[:1000] = np.nextafter(2.0, 0.0) * np.exp2(rng.integers(-8, 8, 1000))
+    b[1000:2000] = np.exp2(rng.integers(-8, 8, 1000))
+    bad = lib.orc_check_rcp_div(a.ctypes.data_as(C.c_void_p), b.ctypes.data_as(C.c_void_p), n)
+    assert bad == 0

@@ -196,6 +196,8 @@ static Rec compile_rec(const tp_elem& e) {
             r.h.kind = DK_EXACT_SBEND;
             r.h.order = uint8_t(e.max_order);
             r.w[eb::IRHO] = irho;
+            r.w[eb::IRHO_INV] = 1.0 / irho;
+            if (std::isnormal(irho) && std::isnormal(r.w[eb::IRHO_INV])) r.h.flags |= RF_RCP_IRHO;
             r.w[eb::GK] = e.gk;
             if (e.e1 != 0.0) {
                 r.h.flags |= RF_YROT_IN;

@@ -62,6 +62,7 @@ enum DevErr : int32_t {
 
 // Kernel launchers (tp_track.cu, compiled once with and once without FMA
 // contraction).  Return a cudaError_t value.
+constexpr int kTrackMaxBlock = 128;  // launch bound of the tracking kernels
 int launch_track_fast(const TrackArgs& a, int grid, int block, int ppt, size_t smem, void* stream);
 int launch_track_strict(const TrackArgs& a, int grid, int block, int ppt, size_t smem, void* stream);
 int occupancy_track_fast(int block, int ppt, size_t smem, int* blocks_per_sm);

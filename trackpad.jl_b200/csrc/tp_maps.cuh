@@ -114,14 +114,13 @@ __device__ __noinline__ void multipole(P6& s, const double* w, int nsteps, doubl
     const double L1b = L1 * beti, L2b = L2 * beti;
     DCache c;
     make_cache(s, beti, c);
-    for (int st = 0; st < nsteps; ++st) {
-        drift<EXACT>(s, L1, L1b, c);
-        thin_kick<M>(s, pa, pb, K1);
-        drift<EXACT>(s, L2, L2b, c);
-        thin_kick<M>(s, pa, pb, K2);
-        drift<EXACT>(s, L2, L2b, c);
-        thin_kick<M>(s, pa, pb, K1);
-        drift<EXACT>(s, L1, L1b, c);
+    // D(L1) K(K1) D(L2) K(K2) D(L2) K(K1) D(L1) per step, as one loop (code size).
+#pragma unroll 1
+    for (int k = 0; k < 4 * nsteps; ++k) {
+        const int j = k & 3;
+        const bool outer = (j == 0) || (j == 3);
+        drift<EXACT>(s, outer ? L1 : L2, outer ? L1b : L2b, c);
+        if (j != 3) thin_kick<M>(s, pa, pb, j == 1 ? K2 : K1);
     }
 }
 
@@ -295,13 +294,34 @@ __device__ __forceinline__ void body_one(P6& r, double irho, double L, double Lb
     r.px = px_new;
 }
 
+// a / b from y = RN(1/b) by Markstein's sequence: q = RN(a*y), r = a - b*q
+// (exact with an FMA), RN(q + r*y) is the correctly rounded quotient a/b
+// (P. Markstein, IBM J. Res. Dev. 34(1), 1990; Theorem 8.10 of "IA-64 and
+// Elementary Functions").  The identity needs b, y and the quotient in the
+// normal range; outside it (and for a = 0, inf or NaN) the IEEE division runs.
+// Finite normal number (device code must not call std::isnormal).
+__device__ __forceinline__ bool is_normal(double v) {
+    const double av = fabs(v);
+    return av >= 2.2250738585072014e-308 && av <= 1.7976931348623157e308;
+}
+
+__device__ __forceinline__ double div_rcp(double a, double b, double y) {
+    double q = __dmul_rn(a, y);
+    double r = fma(-q, b, a);
+    double q1 = fma(r, y, q);
+    double aq = fabs(q);
+    if (!(aq > 1e-280 && aq < 1e280)) q1 = a / b;
+    return q1;
+}
+
 // Consecutive exact_bend_body calls with no kick in between.  py and delta are
 // unchanged by the body, so d2 = pxyz(dp1, 0, py) is the same for every call,
 // the pz of a call is the pxyz(dp1, px_new, py) of the previous one, and its
 // asin(clamp(px/d2)) is the previous asin(clamp(px_new/d2)).  Carrying them
 // leaves every operation of every call as the reference performs it.
 struct BodyCarry {
-    double dp1sq, pysq, d2, pz, as1;
+    double dp1sq, pysq, d2, d2inv, pz, as1;
+    bool rcp_d2;
 };
 
 __device__ __forceinline__ void body_carry_init(const P6& r, double dp1, BodyCarry& b) {
@@ -309,26 +329,54 @@ __device__ __forceinline__ void body_carry_init(const P6& r, double dp1, BodyCar
     b.pysq = r.py * r.py;
     double v0 = b.dp1sq - 0.0 * 0.0 - b.pysq;
     b.d2 = v0 > 0.0 ? sqrt(v0) : 0.0;
+    b.d2inv = 1.0 / b.d2;
+    b.rcp_d2 = is_normal(b.d2) && is_normal(b.d2inv);
     double v = b.dp1sq - r.px * r.px - b.pysq;
     b.pz = v > 0.0 ? sqrt(v) : 0.0;
     b.as1 = libm::asin(jclamp(r.px / b.d2));
 }
 
-__device__ __forceinline__ void body_carry_step(P6& r, BodyCarry& b, double irho, double L, double Lbeti, double cs,
-                                                double sn, double dp1) {
+// One exact_bend_body call (:869-893) with the carried values.  The three
+// quotients have divisors that are fixed for the whole body (d2, irho), so
+// with normal divisors they use the reciprocal sequence (same bits as the
+// division).
+template <bool RCP_IRHO>
+__device__ __forceinline__ void body_carry_step(P6& r, BodyCarry& b, double irho, double irho_inv, double L,
+                                                double Lbeti, double cs, double sn, double dp1) {
     double pzmx = b.pz - (1.0 + r.x * irho);
     double px_new = r.px * cs + pzmx * sn;
-    double as2 = libm::asin(jclamp(px_new / b.d2));
-    double dasin = L + (b.as1 - as2) / irho;
+    double q2 = b.rcp_d2 ? div_rcp(px_new, b.d2, b.d2inv) : px_new / b.d2;
+    double as2 = libm::asin(jclamp(q2));
+    double das = b.as1 - as2;
+    double dasin = L + (RCP_IRHO ? div_rcp(das, irho, irho_inv) : das / irho);
     double v = b.dp1sq - px_new * px_new - b.pysq;
     double pz_new = v > 0.0 ? sqrt(v) : 0.0;
-    double x_new = (pz_new - pzmx * cs + r.px * sn - 1.0) / irho;
+    double num = pz_new - pzmx * cs + r.px * sn - 1.0;
+    double x_new = RCP_IRHO ? div_rcp(num, irho, irho_inv) : num / irho;
     r.y = r.y + r.py * dasin;
     r.z = r.z + dp1 * dasin - Lbeti;
     r.x = x_new;
     r.px = px_new;
     b.pz = pz_new;
     b.as1 = as2;
+}
+
+template <bool RCP_IRHO>
+__device__ __forceinline__ void body_carry_run(P6& r, const double* w, int nsteps, double irho, double dp1,
+                                               double beti) {
+    const double L1 = w[eb::L1], L2 = w[eb::L2];
+    const double L1b = L1 * beti, L2b = L2 * beti;
+    const double cs1 = w[eb::CS1], sn1 = w[eb::SN1], cs2 = w[eb::CS2], sn2 = w[eb::SN2];
+    const double irho_inv = w[eb::IRHO_INV];
+    BodyCarry b;
+    body_carry_init(r, dp1, b);
+    // Sub-steps L1, L2, L2, L1 of every Yoshida step, as one loop (code size).
+#pragma unroll 1
+    for (int k = 0; k < 4 * nsteps; ++k) {
+        const bool outer = ((k & 3) == 0) || ((k & 3) == 3);
+        body_carry_step<RCP_IRHO>(r, b, irho, irho_inv, outer ? L1 : L2, outer ? L1b : L2b, outer ? cs1 : cs2,
+                                  outer ? sn1 : sn2, dp1);
+    }
 }
 
 // Body of pass!(::ExactSBend) between the entrance and exit wedges (:921-953).
@@ -346,14 +394,8 @@ __device__ __noinline__ void exact_body(P6& r, const double* w, const RecHdr& h,
     const double cs1 = w[eb::CS1], sn1 = w[eb::SN1], cs2 = w[eb::CS2], sn2 = w[eb::SN2];
     if ((h.flags & RF_NOKICK) && !straight) {
         if (h.nsteps <= 0) return;
-        BodyCarry b;
-        body_carry_init(r, dp1, b);
-        for (int st = 0; st < h.nsteps; ++st) {
-            body_carry_step(r, b, irho, L1, L1b, cs1, sn1, dp1);
-            body_carry_step(r, b, irho, L2, L2b, cs2, sn2, dp1);
-            body_carry_step(r, b, irho, L2, L2b, cs2, sn2, dp1);
-            body_carry_step(r, b, irho, L1, L1b, cs1, sn1, dp1);
-        }
+        if (h.flags & RF_RCP_IRHO) body_carry_run<true>(r, w, h.nsteps, irho, dp1, beti);
+        else body_carry_run<false>(r, w, h.nsteps, irho, dp1, beti);
         return;
     }
     const double K1 = w[eb::K1], K2 = w[eb::K2];

@@ -52,7 +52,8 @@ enum RecFlag : uint16_t {
     RF_FC_IN_ZERO = 1u << 11,  // SBend: entrance fringecorr == 0
     RF_FC_OUT_ZERO = 1u << 12, // SBend: exit fringecorr == 0
     RF_BODY_ONE = 1u << 13,  // exact bend with num_int_steps == 0: one body call over L
-    RF_OFF = 1u << 14        // Lorentz boost with mode != 0, Accel with beta^2 <= eps ...: identity
+    RF_OFF = 1u << 14,       // Lorentz boost with mode != 0, Accel with beta^2 <= eps ...: identity
+    RF_RCP_IRHO = 1u << 15   // exact bend: irho and RN(1/irho) are normal numbers (reciprocal division)
 };
 
 // Two header words.  `words` is the record length including the header.
@@ -87,7 +88,8 @@ enum {
     EC_IN = 14, ES_IN = 15, ES2_IN = 16, ETH_IN = 17, ETHH_IN = 18,     // bend_edge(-e1): c, s, sin(2t), t, t/h
     EC_OUT = 19, ES_OUT = 20, ES2_OUT = 21, ETH_OUT = 22, ETHH_OUT = 23, // bend_edge(-e2)
     PA = 24, PB = 28,
-    WORDS = 32
+    IRHO_INV = 32,                              // RN(1/irho) for the exact quotient by irho
+    WORDS = 33
 };
 }
 namespace rf { enum { LH = 0, NV = 1, W = 2, LAG = 3, PHILAG = 4, WORDS = 5 }; }

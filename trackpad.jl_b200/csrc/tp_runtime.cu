@@ -598,7 +598,7 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     int schedule = o.schedule ? o.schedule : (nturns > 1 ? 2 : 1);
     a.refill = schedule == 2 ? 1 : 0;
     int block = o.block_size > 0 ? o.block_size : 128;
-    block = std::max(32, std::min(256, block / 32 * 32));
+    block = std::max(32, std::min(kTrackMaxBlock, block / 32 * 32));
     const bool strict = o.fp_contract == 0;
     int bps = 0;
     int oerr = strict ? occupancy_track_strict(block, 1, smem, &bps) : occupancy_track_fast(block, 1, smem, &bps);
@@ -856,7 +856,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     a.beti_v = b->beti_v;
     a.nelem_v = b->nelem_v;
     a.nvar = nvar;
-    int block = o.block_size > 0 ? std::max(32, std::min(256, o.block_size / 32 * 32)) : 128;
+    int block = o.block_size > 0 ? std::max(32, std::min(kTrackMaxBlock, o.block_size / 32 * 32)) : 128;
     int bps = 0;
     int oerr = strict ? occupancy_track_strict(block, 1, 0, &bps) : occupancy_track_fast(block, 1, 0, &bps);
     if (oerr != 0 || bps <= 0) bps = 1;

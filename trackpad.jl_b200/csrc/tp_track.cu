@@ -34,7 +34,16 @@ namespace TP_NS {
 
 using namespace tp::dev;
 
-constexpr int kMaxBlock = 256;
+// 128-thread blocks, at least 5 resident per SM: at most 102 registers per
+// thread (measured fastest on B200 among 128/4, 128/5, 128/6, 128/8 and
+// 64/256-thread blocks; fewer registers spill in the exact-bend maps).
+#ifndef TP_MAX_BLOCK
+#define TP_MAX_BLOCK 128
+#endif
+#ifndef TP_MIN_BLOCKS
+#define TP_MIN_BLOCKS 5
+#endif
+constexpr int kMaxBlock = TP_MAX_BLOCK;
 constexpr long long kTmaSpinLimit = 1ll << 22;  // bounded mbarrier wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -197,7 +206,7 @@ __device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, doubl
 }
 
 template <bool EXACT, bool REFILL>
-__global__ void __launch_bounds__(kMaxBlock) track_single(TrackArgs a) {
+__global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_single(TrackArgs a) {
     extern __shared__ __align__(16) double smem[];
     __shared__ __align__(8) uint64_t mbar;
     const double* tab = a.table;
@@ -235,7 +244,7 @@ __global__ void __launch_bounds__(kMaxBlock) track_single(TrackArgs a) {
 // Batched: warps take 32-particle tiles (variant, first particle) in variant
 // order; tile t of variant v covers particles poff[v] + 32*(t - tile_off[v]).
 template <bool EXACT>
-__global__ void __launch_bounds__(kMaxBlock) track_batched(TrackArgs a, const int64_t* tile_off) {
+__global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_batched(TrackArgs a, const int64_t* tile_off) {
     const int lane = threadIdx.x & 31;
     unsigned long long passes = 0;
     const int64_t ntiles = tile_off[a.nvar];
