@@ -1,0 +1,197 @@
+"""
+    TrackPadB200Ext
+
+Package extension of TrackPad.jl that runs `linepass!` / `ringpass!` on a B200
+through libtrackpad_b200.so (C ABI: include/trackpad_b200.h).  It adds methods
+for device arrays (`CuMatrix{Float64}` coordinates, `CuVector{Int}` flags) and a
+`B200()` backend tag for host arrays; the CPU methods of TrackPad are untouched.
+
+Registration in TrackPad's Project.toml (beside TrackPadCUDAExt):
+    [weakdeps]    CUDA = "052768ef-5323-5732-b1bb-66c8b64840ba"
+    [extensions]  TrackPadB200Ext = "CUDA"
+and set ENV["TRACKPAD_B200_LIB"] to the path of libtrackpad_b200.so.
+"""
+module TrackPadB200Ext
+
+using TrackPad
+using TrackPad: Lattice, Beam, AbstractElement, TimeVaryingElement, TimeContext, materialize, beti
+using CUDA
+
+const LIB = get(ENV, "TRACKPAD_B200_LIB", "libtrackpad_b200.so")
+
+# --- C structs (field order and types as in include/trackpad_b200.h) ---------
+struct TpElem
+    kind::Int32; max_order::Int32; num_int_steps::Int32
+    fringe_bend_entrance::Int32; fringe_bend_exit::Int32; misalign_index::Int32
+    iparam::NTuple{2,Int32}
+    L::Float64; k::Float64; angle::Float64; e1::Float64; e2::Float64
+    fint1::Float64; fint2::Float64; gap::Float64; gk::Float64
+    polynom_a::NTuple{4,Float64}; polynom_b::NTuple{4,Float64}; kick_angle::NTuple{2,Float64}
+    volt::Float64; freq::Float64; h::Float64; lag::Float64; philag::Float64; energy::Float64
+    param::NTuple{8,Float64}
+end
+
+struct TpMisalign
+    t1::NTuple{6,Float64}; t2::NTuple{6,Float64}; r1::NTuple{36,Float64}; r2::NTuple{36,Float64}
+end
+
+struct TpOpts
+    size::Int32; exact_hamiltonian::Int32; device_pointers::Int32; fp_contract::Int32
+    block_size::Int32; ppt::Int32; schedule::Int32; reserved0::Int32
+    aperture_x::Float64; aperture_y::Float64; stream::Ptr{Cvoid}
+end
+
+const TP_KIND = Dict{DataType,Int32}(
+    Marker => 0, Drift => 1, Quadrupole => 2, Sextupole => 3, Octupole => 4, ThinMultipole => 5,
+    SBend => 6, ExactSBend => 7, RFCavity => 8, Solenoid => 9, Corrector => 10, Translation => 11,
+    YRotation => 12, CrabCavity => 13, AccelCavity => 14, LongitudinalRFMap => 15, LorentzBoost => 16,
+    InvLorentzBoost => 17, SpaceCharge => 18, DriftSC => 19, QuadrupoleSC => 20, SextupoleSC => 21,
+    OctupoleSC => 22, SBendSC => 23, StrongThinGaussianBeam => 24)
+
+check(st, what) = st == 0 || error("$what: " * unsafe_string(ccall((:tp_strerror, LIB), Cstring, (Cint,), st)) *
+                                   " (" * unsafe_string(ccall((:tp_last_error_string, LIB), Cstring, ())) * ")")
+
+field(e, s, default) = hasproperty(e, s) ? Float64(getproperty(e, s)) : default
+vec4(e, s) = hasproperty(e, s) ? NTuple{4,Float64}(getproperty(e, s)) : (0.0, 0.0, 0.0, 0.0)
+
+_rf_k(rf::RFCavity) = 2pi * rf.freq / 2.99792458e8
+_rf_k(rf) = hasproperty(rf, :k) ? Float64(rf.k) : 0.0
+_rf_h(rf::CrabCavity) = 1.0
+_rf_h(rf) = hasproperty(rf, :h) ? Float64(rf.h) : 1.0
+
+"""Pack one TrackPad element into the C record (fields by reference name)."""
+function pack(e::AbstractElement, mis_index::Int32)
+    T = typeof(e).name.wrapper
+    kind = get(TP_KIND, T, Int32(-1))
+    kind < 0 && throw(ArgumentError("element $(T) has no device implementation"))
+    k = e isa Quadrupole ? e.k1 : e isa Sextupole ? e.k2 : e isa Octupole ? e.k3 : 0.0
+    p = zeros(8); ip = (Int32(0), Int32(0))
+    if e isa Solenoid; p[1] = e.ks
+    elseif e isa Corrector; p[1] = e.xkick; p[2] = e.ykick
+    elseif e isa Translation; p[1:3] .= (e.dx, e.dy, e.ds)
+    elseif e isa CrabCavity; p[1:4] .= (e.k, e.phi, e.errors[1], e.errors[2])
+    elseif e isa AccelCavity; p[1:2] .= (e.k, e.phis)
+    elseif e isa LongitudinalRFMap; p[1:3] .= (e.alphac, _rf_k(e.rf), _rf_h(e.rf))
+    elseif e isa LorentzBoost; p[1:4] .= (e.angle, e.cosang, 0.0, e.tanang); ip = (Int32(e.mode), Int32(0))
+    elseif e isa InvLorentzBoost; p[1:4] .= (e.angle, e.cosang, e.sinang, 0.0); ip = (Int32(e.mode), Int32(0))
+    elseif e isa Union{QuadrupoleSC,SextupoleSC,OctupoleSC}; p[1:4] .= (e.k0, e.k1, e.k2, e.k3)
+    elseif e isa StrongThinGaussianBeam; p[1:5] .= (e.amplitude, e.rmssizex, e.rmssizey, e.xoffset, e.yoffset)
+    end
+    TpElem(kind, Int32(hasproperty(e, :max_order) ? e.max_order : 0),
+           Int32(hasproperty(e, :num_int_steps) ? e.num_int_steps : 0),
+           Int32(hasproperty(e, :fringe_bend_entrance) ? e.fringe_bend_entrance : 0),
+           Int32(hasproperty(e, :fringe_bend_exit) ? e.fringe_bend_exit : 0), mis_index, ip,
+           field(e, :L, 0.0), Float64(k), field(e, :angle, 0.0), field(e, :e1, 0.0), field(e, :e2, 0.0),
+           field(e, :fint1, 0.0), field(e, :fint2, 0.0), field(e, :gap, 0.0), field(e, :gk, 0.0),
+           vec4(e, :polynom_a), vec4(e, :polynom_b),
+           hasproperty(e, :kick_angle) ? NTuple{2,Float64}(e.kick_angle) : (0.0, 0.0),
+           field(e, :volt, 0.0), field(e, :freq, 0.0), field(e, :h, 0.0), field(e, :lag, 0.0),
+           field(e, :philag, 0.0), field(e, :energy, 0.0), NTuple{8,Float64}(p))
+end
+
+misaligned(e) = hasproperty(e, :t1) && !(iszero(e.t1) && iszero(e.t2) && iszero(e.r1) && iszero(e.r2))
+
+"""Compile a Lattice into a tp_lattice handle (freed by a finalizer)."""
+mutable struct DeviceLattice
+    handle::Ptr{Cvoid}
+end
+
+function DeviceLattice(lat::Lattice)
+    elems = TpElem[]; mis = TpMisalign[]
+    for e in lat.elements
+        b = e isa TimeVaryingElement ? e.base : e
+        idx = Int32(-1)
+        if misaligned(b)
+            push!(mis, TpMisalign(Tuple(b.t1), Tuple(b.t2), Tuple(vec(b.r1)), Tuple(vec(b.r2))))
+            idx = Int32(length(mis) - 1)
+        end
+        push!(elems, pack(b, idx))
+    end
+    h = Ref{Ptr{Cvoid}}(C_NULL)
+    GC.@preserve elems mis begin
+        check(ccall((:tp_lattice_create, LIB), Cint, (Ptr{TpElem}, Int64, Ptr{TpMisalign}, Int64, Ref{Ptr{Cvoid}}),
+                    elems, length(elems), isempty(mis) ? C_NULL : mis, length(mis), h), "tp_lattice_create")
+    end
+    d = DeviceLattice(h[])
+    finalizer(x -> ccall((:tp_lattice_destroy, LIB), Cint, (Ptr{Cvoid},), x.handle), d)
+    d
+end
+
+"""Evaluate the timed fields of every turn into the library's per-turn schedule
+(materialize of src/time_dependence.jl, once per element per turn)."""
+function set_schedule!(d::DeviceLattice, lat::Lattice, time, dt_turn, turn0, nturns)
+    names = Dict(:L => 0, :k1 => 1, :k2 => 1, :k3 => 1, :angle => 2, :e1 => 3, :e2 => 4, :volt => 5,
+                 :freq => 6, :lag => 7, :philag => 8, :energy => 9, :num_int_steps => 10)
+    fields = Int32[]; cols = Tuple{Int,Symbol}[]
+    for (i, e) in enumerate(lat.elements)
+        e isa TimeVaryingElement || continue
+        for s in keys(e.updates)
+            push!(fields, Int32(i - 1), Int32(names[s])); push!(cols, (i, s))
+        end
+    end
+    isempty(cols) && return
+    vals = zeros(Float64, length(cols), nturns)
+    for t in 1:nturns
+        ctx = TimeContext(Float64(time + (t - 1) * dt_turn); turn = turn0 + t - 1)
+        for (j, (i, s)) in enumerate(cols)
+            vals[j, t] = Float64(getproperty(materialize(lat.elements[i], ctx), s))
+        end
+    end
+    check(ccall((:tp_lattice_set_schedule, LIB), Cint, (Ptr{Cvoid}, Ptr{Int32}, Int32, Int32, Int32, Ptr{Float64}),
+                d.handle, fields, length(cols), turn0, nturns, vals), "tp_lattice_set_schedule")
+end
+
+const CTX = Ref{Ptr{Cvoid}}(C_NULL)
+function context()
+    if CTX[] == C_NULL
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:tp_ctx_create, LIB), Cint, (Cint, Ref{Ptr{Cvoid}}), CUDA.device().handle, h), "tp_ctx_create")
+        CTX[] = h[]
+    end
+    CTX[]
+end
+
+opts(device::Bool; aperture = 0.0) =
+    TpOpts(Int32(sizeof(TpOpts)), 1, device ? 1 : 0, 0, 0, 0, 0, 0, aperture, aperture,
+           device ? Ptr{Cvoid}(CUDA.stream().handle) : C_NULL)
+
+"""ringpass! on the GPU for device arrays: coords is N x 6 (column-major, as on the CPU)."""
+function TrackPad.ringpass!(coords::CuMatrix{Float64}, lat::Lattice, beam::Beam{Float64},
+                            lost_flags::CuVector{Int}, nturns::Int; time::Real = 0.0, dt_turn::Real = 0.0,
+                            turn::Integer = 0, aperture::Real = 0.0)
+    size(coords, 2) == 6 || throw(ArgumentError("coords must be N x 6"))
+    d = DeviceLattice(lat)
+    set_schedule!(d, lat, time, dt_turn, turn, max(nturns, 1))
+    o = Ref(opts(true; aperture = Float64(aperture)))
+    check(ccall((:tp_ringpass, LIB), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, CuPtr{Float64}, Int64, CuPtr{Int64}, Ptr{Int32}, Ptr{Int32}, Float64, Int32,
+                 Float64, Float64, Int32, Ref{TpOpts}),
+                context(), d.handle, coords, size(coords, 1), lost_flags, C_NULL, C_NULL, beti(beam), nturns,
+                time, dt_turn, turn, o), "tp_ringpass")
+    nothing
+end
+
+TrackPad.linepass!(coords::CuMatrix{Float64}, lat::Lattice, beam::Beam{Float64}, lost_flags::CuVector{Int};
+                   time::Real = 0.0, turn::Integer = 0, aperture::Real = 0.0) =
+    TrackPad.ringpass!(coords, lat, beam, lost_flags, 1; time = time, turn = turn, aperture = aperture)
+
+"""Backend tag: B200() runs host arrays through the device (copies in and out)."""
+struct B200 end
+
+function TrackPad.ringpass!(::B200, coords::Matrix{Float64}, lat::Lattice, beam::Beam{Float64},
+                            lost_flags::Vector{Int}, nturns::Int; time::Real = 0.0, dt_turn::Real = 0.0,
+                            turn::Integer = 0, aperture::Real = 0.0)
+    d = DeviceLattice(lat)
+    set_schedule!(d, lat, time, dt_turn, turn, max(nturns, 1))
+    o = Ref(opts(false; aperture = Float64(aperture)))
+    GC.@preserve coords lost_flags begin
+        check(ccall((:tp_ringpass, LIB), Cint,
+                    (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}, Int64, Ptr{Int64}, Ptr{Int32}, Ptr{Int32}, Float64, Int32,
+                     Float64, Float64, Int32, Ref{TpOpts}),
+                    context(), d.handle, coords, size(coords, 1), lost_flags, C_NULL, C_NULL, beti(beam), nturns,
+                    time, dt_turn, turn, o), "tp_ringpass")
+    end
+    nothing
+end
+
+end # module
