@@ -353,6 +353,30 @@ TP_API int tp_one_turn_jacobian(tp_ctx* ctx, const tp_lattice* lat,
                                 const tp_opts* opts);
 
 /* ------------------------------------------------------------------------- */
+/* Allocation-free tracking                                                   */
+/* ------------------------------------------------------------------------- */
+/* No counterpart in the reference.  ringpass! for callers that cannot let a
+ * library allocate device memory (a memory pool that owns the whole device,
+ * an allocation-free real-time loop, code that must not let cudaMalloc or
+ * cudaFree synchronise the device): the same tracking kernel as tp_ringpass,
+ * with its scratch (work and pass counters, error word, element table) in a
+ * fixed device array of the library instead of allocated buffers.
+ *   * all data pointers are device pointers on the current device; the call
+ *     runs on `stream` (NULL: the default stream) and returns when it is done;
+ *   * the element table may hold at most 16384 words (128 KiB, about 1400
+ *     DBA-type elements); larger tables give TP_ERANGE, lattices with
+ *     misalignment rows or a per-turn schedule give TP_EUNSUPPORTED;
+ *   * the array (about 128 KiB) stays allocated on every GPU that loads the
+ *     library until the process exits, and every call shares it: calls that
+ *     overlap on the GPU race with each other;
+ *   * the first call on a device looks up the array's address there; make it
+ *     before any stream capture.
+ * Always the exact drift and no FMA contraction (tp_opts defaults). */
+TP_API int tp_ringpass_noalloc(const tp_lattice* lat, double* coords, int64_t n, int64_t* lost_flags,
+                               int32_t* lost_turn, int32_t* lost_elem, double beti, int32_t nturns,
+                               int32_t turn0, double aperture_x, double aperture_y, void* stream);
+
+/* ------------------------------------------------------------------------- */
 /* Diagnostics                                                                */
 /* ------------------------------------------------------------------------- */
 /* Measured FP64 fused-multiply-add throughput of the device (TFLOP/s, 2 FLOPs

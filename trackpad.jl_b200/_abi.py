@@ -131,6 +131,8 @@ _SIGS = {
                                               P, P, P, C.c_int32, P, P, P]),
     "tp_one_turn_jacobian": (C.c_int, [P, P, P, C.c_int64, C.c_double, C.c_int32, C.c_int32, P, P, P]),
     "tp_probe_fp64_peak": (C.c_int, [P, C.POINTER(C.c_double)]),
+    "tp_ringpass_noalloc": (C.c_int, [P, P, C.c_int64, P, P, P, C.c_double, C.c_int32, C.c_int32, C.c_double,
+                                      C.c_double, P]),
 }
 
 _lib = None

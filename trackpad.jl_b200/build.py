@@ -45,6 +45,7 @@ def build(verbose=False, ptxas_info=False):
         ("tp_runtime.o", "tp_runtime.cu", ["-fmad=false"]),
         ("tp_adjoint.o", "tp_adjoint.cu", ["-fmad=true"]),
         ("tp_compile.o", "tp_compile.cpp", ["-fmad=false", "-x", "cu"]),
+        ("tp_noalloc.o", "tp_noalloc.cu", ["-fmad=false"]),
     ]
     objs = []
     log = []

@@ -68,4 +68,17 @@ int launch_track_strict(const TrackArgs& a, int grid, int block, int ppt, size_t
 int occupancy_track_fast(int block, int ppt, size_t smem, int* blocks_per_sm);
 int occupancy_track_strict(int block, int ppt, size_t smem, int* blocks_per_sm);
 
+// Read-only view of a lattice's compiled program (tp_runtime.cu).
+struct LatticeView {
+    const double* program;  // host copy of the compiled table
+    size_t words;
+    int32_t nelem;
+    bool has_schedule;
+    bool has_misalignment;
+};
+void lattice_view(const tp_lattice* lat, LatticeView* out);
+
+// Set the text returned by tp_last_error_string on this thread.
+void set_last_error(const std::string& msg);
+
 }  // namespace tp

@@ -292,6 +292,20 @@ int check_device_error(tp_ctx* c) {
 
 }  // namespace
 
+namespace tp {
+
+void lattice_view(const tp_lattice* lat, LatticeView* out) {
+    out->program = lat->program.data();
+    out->words = lat->program.size();
+    out->nelem = int32_t(lat->elems.size());
+    out->has_schedule = lat->has_sched;
+    out->has_misalignment = !lat->mis.empty();
+}
+
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+}  // namespace tp
+
 // ===========================================================================
 // C ABI
 // ===========================================================================
