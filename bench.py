@@ -164,6 +164,12 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+# DRAM bytes per particle of one tracking launch: ncu capture of track_single on
+# the DBA ring, 69,632 particles x 10 turns (5.425 MB read + written).  Traffic
+# grows with the particle count (the table lives in shared memory).
+DRAM_BYTES_PER_PARTICLE = 5.425152e6 / 69632
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -276,7 +282,9 @@ def main():
                        "elements": len(lat), "l2": "flushed between timed steps (256 MiB write)",
                        "fp": "FMA contraction" if args.contract else "no FMA contraction (reference operation order)"},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": DRAM_BYTES_PER_PARTICLE * n,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on "
+                                           "69,632 particles x 10 turns, scaled by particles",
                          "peak_source": "measured FP64 FMA throughput of this device (tp_probe_fp64_peak)",
                          "flops_per_launch": flops / args.steps, "kernel_ms": k_ms},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
