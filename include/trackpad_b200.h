@@ -338,6 +338,25 @@ TP_API int tp_ringpass_adjoint_batched(tp_ctx* ctx, tp_batch* b,
                                        double* loss_out, double* grad_out,
                                        const tp_opts* opts);
 
+/* Statistics of the last adjoint or Jacobian call on this host thread (no
+ * reference counterpart).  The reverse sweep rebuilds each K-turn segment
+ * with the maps' time-reversed forms; reconstruction_error is the largest
+ * absolute difference, over survivors and segment starts, between a rebuilt
+ * state and the stored checkpoint. */
+typedef struct tp_adjoint_stats {
+    int32_t checkpoint_every;     /* K used                                       */
+    int32_t segments;             /* ceil(nturns / K)                             */
+    int64_t checkpoint_bytes;     /* device memory of the stored states           */
+    int64_t particles;            /* particles in the launch                      */
+    double units;                 /* particle*element*turns of the forward pass   */
+    double forward_ms;            /* device time of the forward (checkpointing) pass */
+    double reverse_ms;            /* device time of the reverse sweep             */
+    double reconstruction_error;
+    int32_t launches;
+    int32_t reserved;
+} tp_adjoint_stats;
+TP_API int tp_last_adjoint_stats(tp_adjoint_stats* out);
+
 /* ------------------------------------------------------------------------- */
 /* One-turn Jacobian and symplecticity                                        */
 /* ------------------------------------------------------------------------- */

@@ -79,6 +79,14 @@ class TpLossSpec(C.Structure):
     _fields_ = [("kind", C.c_int32), ("reserved", C.c_int32), ("sigma", C.c_double), ("lost_weight", C.c_double)]
 
 
+class TpAdjointStats(C.Structure):
+    _fields_ = [
+        ("checkpoint_every", C.c_int32), ("segments", C.c_int32), ("checkpoint_bytes", C.c_int64),
+        ("particles", C.c_int64), ("units", C.c_double), ("forward_ms", C.c_double), ("reverse_ms", C.c_double),
+        ("reconstruction_error", C.c_double), ("launches", C.c_int32), ("reserved", C.c_int32),
+    ]
+
+
 def elem_from_dict(d):
     """Fill a TpElem from a dict with reference field names (kind given by name)."""
     e = TpElem()
@@ -130,6 +138,7 @@ _SIGS = {
     "tp_ringpass_adjoint_batched": (C.c_int, [P, P, P, P, P, P, C.c_int32, C.c_double, C.c_double, C.c_int32,
                                               P, P, P, C.c_int32, P, P, P]),
     "tp_one_turn_jacobian": (C.c_int, [P, P, P, C.c_int64, C.c_double, C.c_int32, C.c_int32, P, P, P]),
+    "tp_last_adjoint_stats": (C.c_int, [C.POINTER(TpAdjointStats)]),
     "tp_probe_fp64_peak": (C.c_int, [P, C.POINTER(C.c_double)]),
     "tp_ringpass_noalloc": (C.c_int, [P, P, C.c_int64, P, P, P, C.c_double, C.c_int32, C.c_int32, C.c_double,
                                       C.c_double, P]),

@@ -43,7 +43,7 @@ def build(verbose=False, ptxas_info=False):
         ("tp_track_fast.o", "tp_track.cu", ["-DTP_NS=fast", "-fmad=true"]),
         ("tp_track_strict.o", "tp_track.cu", ["-DTP_NS=strict", "-fmad=false"]),
         ("tp_runtime.o", "tp_runtime.cu", ["-fmad=false"]),
-        ("tp_adjoint.o", "tp_adjoint.cu", ["-fmad=true"]),
+        ("tp_adjoint.o", "tp_adjoint.cu", ["-fmad=false"]),
         ("tp_compile.o", "tp_compile.cpp", ["-fmad=false", "-x", "cu"]),
         ("tp_noalloc.o", "tp_noalloc.cu", ["-fmad=false"]),
     ]

@@ -49,6 +49,7 @@ struct TrackArgs {
     const int64_t* toff;
     const double* beti_v;
     const int32_t* nelem_v;
+    const int64_t* sched_v;     // batched: per variant word offset into `sched` (-1: none), stride, first turn, turns
     int32_t nvar;
     int32_t smem_words;         // words staged into shared memory per block
 };
@@ -77,6 +78,37 @@ struct LatticeView {
     bool has_misalignment;
 };
 void lattice_view(const tp_lattice* lat, LatticeView* out);
+
+// Everything the adjoint and Jacobian paths read from a lattice (tp_runtime.cu).
+struct LatticeHost {
+    const tp_elem* elems;
+    int32_t nelem;
+    const double* program;    // compiled table (scheduled elements are stubs)
+    size_t words;
+    const int32_t* rec_off;   // word offset of each element's record
+    const double* sched;      // per-turn records of scheduled elements (null without schedule)
+    size_t sched_words;
+    int32_t sched_stride, sched_turn0, sched_nturns;
+    bool has_schedule;
+    int64_t nmis;
+};
+void lattice_host(const tp_lattice* lat, LatticeHost* out);
+
+// Context properties and per-context device scratch (tp_runtime.cu).  Scratch
+// slot `slot` grows to at least `bytes` and is kept until the context is
+// destroyed.
+struct CtxHost {
+    int device;
+    int sm_count;
+    size_t smem_optin;
+    void* stream;
+};
+void ctx_host(const tp_ctx* c, CtxHost* out);
+tp_stats* ctx_stats(tp_ctx* c);
+constexpr int kCtxScratchSlots = 12;
+int ctx_scratch(tp_ctx* c, int slot, size_t bytes, void** out);
+// The lattices of a batch in variant order.
+void batch_lattices(const tp_batch* b, std::vector<const tp_lattice*>* out);
 
 // Set the text returned by tp_last_error_string on this thread.
 void set_last_error(const std::string& msg);

@@ -90,6 +90,10 @@ struct tp_batch {
     std::vector<int32_t> h_nelem;
     std::vector<int64_t> h_mis_off;    // misalignment row offset per variant
     size_t table_words = 0;
+    double* sched = nullptr;           // concatenated per-turn schedule tables
+    int64_t* sched_v = nullptr;        // per variant: word offset (-1: none), stride, first turn, turns
+    std::vector<uint64_t> h_ver;       // lattice versions the device tables were built from
+    std::vector<int64_t> h_sched_v;
     // cached CUDA graph of the launch sequence
     cudaGraphExec_t graph = nullptr;
     std::vector<int64_t> g_poff;
@@ -97,6 +101,7 @@ struct tp_batch {
     double g_limx = 0, g_limy = 0;
     const void* g_coords = nullptr;
     const void* g_lost = nullptr;
+    const void* g_table = nullptr;
 };
 
 struct tp_ctx {
@@ -117,6 +122,9 @@ struct tp_ctx {
     uint8_t* alive0 = nullptr;
     int64_t cap = 0;
     tp_stats stats{};
+    // grow-only device scratch of the adjoint and Jacobian paths
+    void* scr[kCtxScratchSlots] = {};
+    size_t scr_bytes[kCtxScratchSlots] = {};
 };
 
 namespace {
@@ -302,6 +310,52 @@ void lattice_view(const tp_lattice* lat, LatticeView* out) {
     out->has_misalignment = !lat->mis.empty();
 }
 
+void lattice_host(const tp_lattice* lat, LatticeHost* out) {
+    out->elems = lat->elems.data();
+    out->nelem = int32_t(lat->elems.size());
+    out->program = lat->program.data();
+    out->words = lat->program.size();
+    out->rec_off = lat->rec_off.data();
+    out->has_schedule = lat->has_sched;
+    out->sched = lat->has_sched ? lat->sched_table.data() : nullptr;
+    out->sched_words = lat->has_sched ? lat->sched_table.size() : 0;
+    out->sched_stride = lat->sched_stride;
+    out->sched_turn0 = lat->sturn0;
+    out->sched_nturns = lat->snturns;
+    out->nmis = int64_t(lat->mis.size());
+}
+
+void ctx_host(const tp_ctx* c, CtxHost* out) {
+    out->device = c->device;
+    out->sm_count = c->sm_count;
+    out->smem_optin = c->smem_optin;
+    out->stream = c->stream;
+}
+
+tp_stats* ctx_stats(tp_ctx* c) { return &c->stats; }
+
+int ctx_scratch(tp_ctx* c, int slot, size_t bytes, void** out) {
+    if (slot < 0 || slot >= kCtxScratchSlots) return set_err(TP_EINVAL, "scratch slot out of range");
+    bytes = std::max<size_t>(bytes, 256);
+    if (c->scr_bytes[slot] < bytes) {
+        if (c->scr[slot]) {
+            cudaStreamSynchronize(c->stream);
+            cudaFree(c->scr[slot]);
+        }
+        c->scr[slot] = nullptr;
+        c->scr_bytes[slot] = 0;
+        if (cudaMalloc(&c->scr[slot], bytes) != cudaSuccess) {
+            cudaGetLastError();
+            return set_err(TP_ENOMEM, "device scratch allocation of " + std::to_string(bytes) + " bytes failed");
+        }
+        c->scr_bytes[slot] = bytes;
+    }
+    *out = c->scr[slot];
+    return TP_OK;
+}
+
+void batch_lattices(const tp_batch* b, std::vector<const tp_lattice*>* out) { *out = b->lats; }
+
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 
 }  // namespace tp
@@ -383,6 +437,7 @@ TP_API int tp_ctx_destroy(tp_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     cudaFree(c->counters); cudaFree(c->err); cudaFree(c->flops_acc);
     cudaFree(c->coords); cudaFree(c->lost); cudaFree(c->lost_turn); cudaFree(c->lost_elem); cudaFree(c->alive0);
+    for (int k = 0; k < kCtxScratchSlots; ++k) cudaFree(c->scr[k]);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -691,26 +746,28 @@ TP_API int tp_ringpass(tp_ctx* c, const tp_lattice* L, double* coords, int64_t n
 // ---------------------------------------------------------------------------
 // Batches
 // ---------------------------------------------------------------------------
-TP_API int tp_batch_create(tp_ctx* c, const tp_lattice* const* lats, int32_t nvar, tp_batch** out) {
-    if (!c || !out || (nvar > 0 && !lats)) return set_err(TP_EINVAL, "null argument");
-    *out = nullptr;
-    if (nvar <= 0) return set_err(TP_EINVAL, "a batch needs at least one lattice");
-    for (int32_t v = 0; v < nvar; ++v) {
-        if (!lats[v]) return set_err(TP_EINVAL, "null lattice in batch");
-        if (lats[v]->has_sched) return set_err(TP_EUNSUPPORTED, "batched tracking of scheduled lattices");
-    }
-    TP_CUDA(cudaSetDevice(c->device));
-    tp_batch* b = new (std::nothrow) tp_batch();
-    if (!b) return set_err(TP_ENOMEM, "host allocation failed");
-    b->nvar = nvar;
-    b->device = c->device;
-    b->lats.assign(lats, lats + nvar);
-    std::vector<double> table;
+// (Re)build the device tables of a batch from its lattices: programs,
+// misalignment rows, per-turn schedules and FLOP prefix tables.
+static void batch_free_tables(tp_batch* b) {
+    cudaFree(b->table); cudaFree(b->toff); cudaFree(b->nelem_v); cudaFree(b->beti_v); cudaFree(b->poff);
+    cudaFree(b->mis); cudaFree(b->prefix); cudaFree(b->prefix_off); cudaFree(b->sched); cudaFree(b->sched_v);
+    b->table = nullptr; b->toff = nullptr; b->nelem_v = nullptr; b->beti_v = nullptr; b->poff = nullptr;
+    b->mis = nullptr; b->prefix = nullptr; b->prefix_off = nullptr; b->sched = nullptr; b->sched_v = nullptr;
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+}
+
+static int batch_build(tp_batch* b) {
+    batch_free_tables(b);
+    const int32_t nvar = b->nvar;
+    std::vector<double> table, sched;
     std::vector<MisalignDev> mis;
     b->h_toff.assign(size_t(nvar) + 1, 0);
     b->h_nelem.assign(size_t(nvar), 0);
+    b->h_ver.assign(size_t(nvar), 0);
+    b->h_sched_v.assign(4 * size_t(nvar), 0);
     for (int32_t v = 0; v < nvar; ++v) {
-        const tp_lattice* L = lats[v];
+        const tp_lattice* L = b->lats[size_t(v)];
+        b->h_ver[size_t(v)] = L->version;
         b->h_toff[size_t(v)] = int64_t(table.size());
         b->h_nelem[size_t(v)] = int32_t(L->elems.size());
         int32_t mbase = int32_t(mis.size());
@@ -729,6 +786,24 @@ TP_API int tp_batch_create(tp_ctx* c, const tp_lattice* const* lats, int32_t nva
             for (int k = 0; k < 36; ++k) { o.r1nz |= m.r1[k] != 0.0; o.r2nz |= m.r2[k] != 0.0; }
             mis.push_back(o);
         }
+        int64_t* sv = &b->h_sched_v[4 * size_t(v)];
+        sv[0] = -1;
+        if (L->has_sched) {
+            sv[0] = int64_t(sched.size());
+            sv[1] = L->sched_stride;
+            sv[2] = L->sturn0;
+            sv[3] = L->snturns;
+            std::vector<double> blk = L->sched_table;
+            if (mbase > 0) {  // misalignment rows inside the per-turn records
+                for (size_t w = 0; w < blk.size();) {
+                    RecHdr* h = reinterpret_cast<RecHdr*>(blk.data() + w);
+                    if (h->words == 0) break;
+                    if (h->flags & RF_MISALIGN) h->aux += mbase;
+                    w += h->words;
+                }
+            }
+            sched.insert(sched.end(), blk.begin(), blk.end());
+        }
     }
     b->h_toff[size_t(nvar)] = int64_t(table.size());
     b->table_words = table.size();
@@ -736,7 +811,7 @@ TP_API int tp_batch_create(tp_ctx* c, const tp_lattice* const* lats, int32_t nva
     std::vector<double> pre_e, pre_l;
     std::vector<int64_t> pre_off(size_t(nvar) + 1, 0);
     for (int32_t v = 0; v < nvar; ++v) {
-        const tp_lattice* L = lats[v];
+        const tp_lattice* L = b->lats[size_t(v)];
         pre_off[size_t(v)] = int64_t(pre_e.size());
         double ae = 0.0, al = 0.0;
         for (size_t i = 0; i < L->elems.size(); ++i) {
@@ -767,8 +842,32 @@ TP_API int tp_batch_create(tp_ctx* c, const tp_lattice* const* lats, int32_t nva
         e = cudaMalloc(&b->mis, mis.size() * sizeof(MisalignDev));
         if (e == cudaSuccess) e = cudaMemcpy(b->mis, mis.data(), mis.size() * sizeof(MisalignDev), cudaMemcpyHostToDevice);
     }
-    if (e != cudaSuccess) {
-        int st = cuda_err(e, "tp_batch_create");
+    if (e == cudaSuccess && !sched.empty()) {
+        e = cudaMalloc(&b->sched, sched.size() * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemcpy(b->sched, sched.data(), sched.size() * sizeof(double), cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&b->sched_v, b->h_sched_v.size() * sizeof(int64_t));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(b->sched_v, b->h_sched_v.data(), b->h_sched_v.size() * sizeof(int64_t), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return cuda_err(e, "batch tables");
+    return TP_OK;
+}
+
+TP_API int tp_batch_create(tp_ctx* c, const tp_lattice* const* lats, int32_t nvar, tp_batch** out) {
+    if (!c || !out || (nvar > 0 && !lats)) return set_err(TP_EINVAL, "null argument");
+    *out = nullptr;
+    if (nvar <= 0) return set_err(TP_EINVAL, "a batch needs at least one lattice");
+    for (int32_t v = 0; v < nvar; ++v) {
+        if (!lats[v]) return set_err(TP_EINVAL, "null lattice in batch");
+    }
+    TP_CUDA(cudaSetDevice(c->device));
+    tp_batch* b = new (std::nothrow) tp_batch();
+    if (!b) return set_err(TP_ENOMEM, "host allocation failed");
+    b->nvar = nvar;
+    b->device = c->device;
+    b->lats.assign(lats, lats + nvar);
+    int st = batch_build(b);
+    if (st != TP_OK) {
         tp_batch_destroy(b);
         return st;
     }
@@ -781,11 +880,7 @@ TP_API int tp_batch_destroy(tp_batch* b) {
     int cur = 0;
     cudaGetDevice(&cur);
     if (b->device >= 0) cudaSetDevice(b->device);
-    if (b->graph) cudaGraphExecDestroy(b->graph);
-    cudaFree(b->table); cudaFree(b->toff); cudaFree(b->nelem_v); cudaFree(b->beti_v); cudaFree(b->poff);
-    cudaFree(b->mis);
-    cudaFree(b->prefix);
-    cudaFree(b->prefix_off);
+    batch_free_tables(b);
     cudaSetDevice(cur);
     cudaGetLastError();
     delete b;
@@ -813,7 +908,21 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     tp_opts o = default_opts(opts_in);
     c->stats = tp_stats{};
     if (n == 0 || nturns == 0) return TP_OK;
+    for (int32_t v = 0; v < nvar; ++v) {
+        const tp_lattice* L = b->lats[size_t(v)];
+        if (L->has_sched && (int64_t(turn0) < L->sturn0 || int64_t(turn0) + nturns > int64_t(L->sturn0) + L->snturns))
+            return set_err(TP_ERANGE, "turns outside the schedule of variant " + std::to_string(v));
+    }
     TP_CUDA(cudaSetDevice(c->device));
+    {   // a member lattice changed (e.g. a new schedule): rebuild the device tables
+        bool stale = false;
+        for (int32_t v = 0; v < nvar; ++v) stale = stale || b->lats[size_t(v)]->version != b->h_ver[size_t(v)];
+        if (stale) {
+            TP_CUDA(cudaDeviceSynchronize());
+            int bst = batch_build(b);
+            if (bst != TP_OK) return bst;
+        }
+    }
     cudaStream_t s = o.stream ? static_cast<cudaStream_t>(o.stream) : c->stream;
     const bool dev = o.device_pointers != 0;
     const bool exact = o.exact_hamiltonian != 0;
@@ -870,6 +979,8 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     a.beti_v = b->beti_v;
     a.nelem_v = b->nelem_v;
     a.nvar = nvar;
+    a.sched = b->sched;
+    a.sched_v = b->sched_v;
     int block = o.block_size > 0 ? std::max(32, std::min(kTrackMaxBlock, o.block_size / 32 * 32)) : 128;
     int bps = 0;
     int oerr = strict ? occupancy_track_strict(block, 1, 0, &bps) : occupancy_track_fast(block, 1, 0, &bps);
@@ -902,7 +1013,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
         // The graph bakes in the argument values; rebuild it when they change.
         bool same = b->graph && b->g_nturns == nturns && b->g_turn0 == turn0 && b->g_exact == int(exact) &&
                     b->g_strict == int(strict) && b->g_limx == a.limx && b->g_limy == a.limy &&
-                    b->g_coords == d_coords && b->g_lost == d_lost &&
+                    b->g_coords == d_coords && b->g_lost == d_lost && b->g_table == b->table &&
                     b->g_poff == std::vector<int64_t>(poff, poff + nvar + 1);
         if (!same) {
             if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
@@ -921,6 +1032,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
             if (ce != cudaSuccess) { b->graph = nullptr; return cuda_err(ce, "cudaGraphInstantiate"); }
             b->g_nturns = nturns; b->g_turn0 = turn0; b->g_exact = int(exact); b->g_strict = int(strict);
             b->g_limx = a.limx; b->g_limy = a.limy; b->g_coords = d_coords; b->g_lost = d_lost;
+            b->g_table = b->table;
             b->g_poff.assign(poff, poff + nvar + 1);
         }
         TP_CUDA(cudaEventRecord(c->ev0, s));

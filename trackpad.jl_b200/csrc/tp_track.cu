@@ -267,7 +267,17 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_batched(TrackA
             more = false;
             return mine < endp ? mine : -1;
         };
-        run_warp<EXACT, false>(a, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next, passes);
+        if (a.sched_v != nullptr && a.sched_v[4 * v] >= 0) {
+            // this variant's per-turn schedule
+            TrackArgs av = a;
+            av.sched = a.sched + a.sched_v[4 * v];
+            av.sched_stride = int32_t(a.sched_v[4 * v + 1]);
+            av.sched_turn0 = int32_t(a.sched_v[4 * v + 2]);
+            av.sched_nturns = int32_t(a.sched_v[4 * v + 3]);
+            run_warp<EXACT, false>(av, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next, passes);
+        } else {
+            run_warp<EXACT, false>(a, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next, passes);
+        }
     }
     if (lane == 0 && passes) atomicAdd(a.passes, passes);
 }

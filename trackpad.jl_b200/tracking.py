@@ -411,9 +411,14 @@ class Batch:
         _abi.check(_abi.lib().tp_batch_create(context(device), hs, len(self.lattices), C.byref(h)), "tp_batch_create")
         self._handle = h
 
-    def ringpass_(self, coords, poff, betis, lost_flags, nturns, *, turn=0, aperture=None, lost_turn=None,
-                  lost_elem=None, exact=True, contract=False, use_graph=True, block_size=0, stream=None):
+    def ringpass_(self, coords, poff, betis, lost_flags, nturns, *, time=0.0, dt_turn=0.0, turn=0, aperture=None,
+                  lost_turn=None, lost_elem=None, exact=True, contract=False, use_graph=True, block_size=0,
+                  stream=None):
+        """ringpass! of every variant in one launch; variant v owns particles
+        poff[v]..poff[v+1].  Time-dependent variants are evaluated per turn."""
         b = _Buffers(coords, lost_flags, lost_turn, lost_elem)
+        for lat in self.lattices:
+            lat.set_schedule(time, dt_turn, turn, max(int(nturns), 1))
         poff = np.ascontiguousarray(poff, dtype=np.int64)
         betis = np.ascontiguousarray(betis, dtype=np.float64)
         if poff.shape != (len(self.lattices) + 1,) or betis.shape != (len(self.lattices),):
@@ -428,12 +433,161 @@ class Batch:
         _abi.check(st, "tp_ringpass_batched")
         b.finish()
 
+    def ringpass_adjoint(self, coords0, poff, betis, lost0, nturns, params, *, sigma, lost_weight=1e3, time=0.0,
+                         dt_turn=0.0, turn=0, aperture=None, exact=True, checkpoint_every=0, stream=None):
+        """Per-variant loss and gradient in one launch (see ringpass_adjoint).
+
+        params[v] lists the parameter elements of variant v.  Returns
+        (loss[nvar], [grad_v for each variant]).
+        """
+        cp, lp, n, dev, keep = _adj_inputs(coords0, lost0)
+        poff = np.ascontiguousarray(poff, dtype=np.int64)
+        betis = np.ascontiguousarray(betis, dtype=np.float64)
+        nv = len(self.lattices)
+        if poff.shape != (nv + 1,) or betis.shape != (nv,) or poff[-1] != n:
+            raise ValueError("poff must have nvar+1 entries ending at N and betis nvar entries")
+        if len(params) != nv:
+            raise ValueError("params needs one list per variant")
+        for lat in self.lattices:
+            lat.set_schedule(time, dt_turn, turn, max(int(nturns), 1))
+        flat = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.int32).reshape(-1) for p in params])
+                                    if nv else np.zeros(0, np.int32), dtype=np.int32)
+        pof = np.zeros(nv + 1, dtype=np.int32)
+        pof[1:] = np.cumsum([len(p) for p in params])
+        loss = np.zeros(nv)
+        grad = np.zeros(max(len(flat), 1))
+        o = _opts(aperture, exact, False, dev is not None, stream=stream)
+        ls = _loss_spec(sigma, lost_weight)
+        st = _abi.lib().tp_ringpass_adjoint_batched(
+            context(self.device), self._handle, cp, poff.ctypes.data_as(C.c_void_p), lp,
+            betis.ctypes.data_as(C.c_void_p), int(nturns), C.c_double(0.0), C.c_double(0.0), int(turn),
+            flat.ctypes.data_as(C.c_void_p), pof.ctypes.data_as(C.c_void_p), C.byref(ls), int(checkpoint_every),
+            loss.ctypes.data_as(C.c_void_p), grad.ctypes.data_as(C.c_void_p), C.byref(o))
+        _abi.check(st, "tp_ringpass_adjoint_batched")
+        return loss, [grad[pof[v]:pof[v + 1]].copy() for v in range(nv)]
+
     def __del__(self):
         if getattr(self, "_handle", None) is not None and _abi._lib is not None:
             try:
                 _abi.lib().tp_batch_destroy(self._handle)
             except Exception:  # pragma: no cover
                 pass
+
+
+# ---------------------------------------------------------------------------
+# Derivatives: adjoint gradient of a beam loss, one-turn Jacobian
+# ---------------------------------------------------------------------------
+def _adj_inputs(coords0, lost0):
+    """(coords pointer, lost pointer, n, device index or None, keep-alive list)."""
+    try:
+        import torch
+        is_t = isinstance(coords0, torch.Tensor)
+    except ImportError:  # pragma: no cover
+        is_t = False
+    if is_t:
+        if not coords0.is_cuda or coords0.dtype != torch.float64 or coords0.dim() != 2 or coords0.shape[1] != 6 \
+                or coords0.stride() != (1, coords0.shape[0]):
+            raise ValueError("device coords0 must be an (N, 6) float64 column-major CUDA view")
+        n = coords0.shape[0]
+        if lost0 is not None and (lost0.dtype != torch.int64 or lost0.shape != (n,) or not lost0.is_contiguous()):
+            raise TypeError("lost0 must be a contiguous int64 CUDA vector of length N")
+        return (C.c_void_p(coords0.data_ptr()), None if lost0 is None else C.c_void_p(lost0.data_ptr()), n,
+                coords0.device.index, [coords0, lost0])
+    c = np.asfortranarray(coords0, dtype=np.float64)
+    if c.ndim != 2 or c.shape[1] != 6:
+        raise ValueError("coords0 must have shape (N, 6)")
+    n = c.shape[0]
+    keep = [c]
+    lp = None
+    if lost0 is not None:
+        l = np.ascontiguousarray(lost0, dtype=np.int64)
+        if l.shape != (n,):
+            raise ValueError("lost0 must have length N")
+        keep.append(l)
+        lp = l.ctypes.data_as(C.c_void_p)
+    return c.ctypes.data_as(C.c_void_p), lp, n, None, keep
+
+
+def _loss_spec(sigma, lost_weight):
+    ls = _abi.TpLossSpec()
+    ls.kind = 0
+    ls.sigma = float(sigma)
+    ls.lost_weight = float(lost_weight)
+    return ls
+
+
+def ringpass_adjoint(coords0, lat, beam, lost0, nturns, params, *, sigma, lost_weight=1e3, time=0.0, dt_turn=0.0,
+                     turn=0, aperture=None, exact=True, checkpoint_every=0, return_state=False, stream=None):
+    """Loss of a tracked beam and its gradient with respect to element strengths.
+
+    loss = mean over the particles that survive `nturns` of (x^2 + y^2)/sigma^2
+           + lost_weight * (lost / alive at start)
+    `params` lists element indices (0-based) of Quadrupoles, Sextupoles or
+    Octupoles; grad[j] = d loss / d k of params[j] (k1, k2 or k3), with the
+    survivor set held fixed.  A time-dependent strength is shifted by the same
+    amount at every turn.  coords0/lost0 are read only (numpy host arrays or
+    CUDA tensors).  Returns (loss, grad), plus (coords, lost_flags) after the
+    forward pass when `return_state` is set.
+    """
+    if not isinstance(lat, Lattice):
+        lat = Lattice(lat)
+    cp, lp, n, dev, keep = _adj_inputs(coords0, lost0)
+    lat.set_schedule(time, dt_turn, turn, max(int(nturns), 1))
+    prm = np.ascontiguousarray(params, dtype=np.int32).reshape(-1)
+    grad = np.zeros(max(len(prm), 1))
+    loss = C.c_double()
+    out_c = out_l = None
+    ocp = olp = None
+    if return_state:
+        if dev is None:
+            out_c = np.zeros((n, 6), order="F")
+            out_l = np.zeros(n, dtype=np.int64)
+            ocp, olp = out_c.ctypes.data_as(C.c_void_p), out_l.ctypes.data_as(C.c_void_p)
+        else:
+            import torch
+            out_c = torch.empty((6, n), dtype=torch.float64, device=f"cuda:{dev}").T
+            out_l = torch.empty(n, dtype=torch.int64, device=f"cuda:{dev}")
+            ocp, olp = C.c_void_p(out_c.data_ptr()), C.c_void_p(out_l.data_ptr())
+    o = _opts(aperture, exact, False, dev is not None, stream=stream)
+    ls = _loss_spec(sigma, lost_weight)
+    st = _abi.lib().tp_ringpass_adjoint(context(dev), lat.handle, cp, n, lp, C.c_double(beti(beam)), int(nturns),
+                                        C.c_double(time), C.c_double(dt_turn), int(turn),
+                                        prm.ctypes.data_as(C.c_void_p), len(prm), C.byref(ls), int(checkpoint_every),
+                                        C.byref(loss), grad.ctypes.data_as(C.c_void_p), ocp, olp, C.byref(o))
+    _abi.check(st, "tp_ringpass_adjoint")
+    if return_state:
+        return loss.value, grad[:len(prm)], out_c, out_l
+    return loss.value, grad[:len(prm)]
+
+
+def one_turn_jacobian(lat, beam, orbits, *, nturns=1, turn=0, time=0.0, dt_turn=0.0, exact=True):
+    """Tangent maps of `nturns` passes about each orbit and their symplecticity.
+
+    The exact counterpart of one_turn_map (src/optics.jl:110-121, finite
+    differences there).  orbits: (n, 6).  Returns (M, err) with M of shape
+    (n, 6, 6) and err[i] = ||M^T J M - J||_max, J = diag(J2, J2, -J2).  An
+    orbit lost on the way gives NaN.
+    """
+    if not isinstance(lat, Lattice):
+        lat = Lattice(lat)
+    orb = np.asfortranarray(np.atleast_2d(orbits), dtype=np.float64)
+    n = orb.shape[0]
+    lat.set_schedule(time, dt_turn, turn, max(int(nturns), 1))
+    jac = np.zeros((n, 36))
+    err = np.zeros(n)
+    o = _opts(None, exact, False, False)
+    st = _abi.lib().tp_one_turn_jacobian(context(), lat.handle, orb.ctypes.data_as(C.c_void_p), n,
+                                         C.c_double(beti(beam)), int(nturns), int(turn),
+                                         jac.ctypes.data_as(C.c_void_p), err.ctypes.data_as(C.c_void_p), C.byref(o))
+    _abi.check(st, "tp_one_turn_jacobian")
+    return np.transpose(jac.reshape(n, 6, 6), (0, 2, 1)), err
+
+
+def adjoint_stats():
+    """Statistics of the last adjoint or Jacobian call on this thread."""
+    st = _abi.TpAdjointStats()
+    _abi.check(_abi.lib().tp_last_adjoint_stats(C.byref(st)), "tp_last_adjoint_stats")
+    return {f: getattr(st, f) for f, _ in st._fields_}
 
 
 def probe_fp64_peak(device=None):
