@@ -5,10 +5,18 @@ entries x turns per second).  Workload (default): the DBA storage ring, 3 GeV
 electrons, 401 elements (20 cells + RF), 1,048,576 Gaussian particles plus a
 512 x 512 dynamic-aperture grid, rectangular aperture 0.02 m.  One step is
 ringpass! over STEP_TURNS turns of that whole beam, restarted from the input
-distribution.  Synthetic, seeded inputs (Philox); no dataset is involved.
+distribution.  Synthetic, seeded inputs (Philox); no dataset is involved.  The
+default line also carries the adjoint/forward time ratio of the gradient
+workload (65,536 particles, 256 turns, 120 k1 + 80 k2).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload dba|fodo|batched]
+                  [--workload dba|fodo|batched|adjoint|batched_adjoint]
+
+  batched          256 DBA variants (4..20 cells, strengths +-2%), 4,096 x U[0.25, 1]
+                   particles each, one CUDA-graph launch per step
+  adjoint          loss + gradient on the DBA ring: 65,536 particles, 256 turns
+  batched_adjoint  64 time-dependent DBA variants (Q1 ramp +1%, RF voltage 5% at a
+                   200-turn period), 16,384 particles each, gradients of every variant
 
 Under torchrun each rank tracks its own beam of the same size (weak scaling,
 no collective on the data path); time is the max over ranks.
@@ -28,6 +36,13 @@ sys.path.insert(0, ROOT)
 
 STEP_TURNS = 10
 L2_FLUSH_BYTES = 256 << 20
+SIGMA_LOSS = 1e-4      # sigma_x of the beam-size loss
+LOST_WEIGHT = 1e3
+
+# DRAM bytes per particle of one tracking launch: ncu capture of track_single on
+# the DBA ring, 69,632 particles x 10 turns (5.425 MB read + written).  Traffic
+# grows with the particle count (the table lives in shared memory).
+DRAM_BYTES_PER_PARTICLE = 5.425152e6 / 69632
 
 
 def parse():
@@ -36,12 +51,15 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="dba", choices=["dba", "fodo", "batched"])
+    p.add_argument("--workload", default="dba", choices=["dba", "fodo", "batched", "adjoint", "batched_adjoint"])
     p.add_argument("--n-gauss", type=int, default=1 << 20)
     p.add_argument("--grid", type=int, default=512)
+    p.add_argument("--turns", type=int, default=0, help="turns per step (0: the workload's default)")
+    p.add_argument("--nvar", type=int, default=0, help="variants of the batched workloads (0: default)")
     p.add_argument("--contract", action="store_true", help="kernels built with FMA contraction")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-adjoint", action="store_true", help="default workload: skip the adjoint ratio")
     return p.parse_args()
 
 
@@ -95,18 +113,44 @@ class Clocks:
                 "samples": len(sm)}
 
 
+# ---------------------------------------------------------------------------
+# Workloads
+# ---------------------------------------------------------------------------
 def workload(args, rank):
     import trackpad_b200.workloads as W
     if args.workload == "fodo":
         lat, beam = W.fodo_ring(), W.fodo_beam()
         coords = W.gaussian(10000, seed=rank)
         return dict(name="FODO ring, 8 cells (32 elements), 1 GeV e-, 10,000 Gaussian particles, aperture 0.05 m",
-                    lat=lat, beam=beam, coords=coords, aperture=0.05, turns=STEP_TURNS)
+                    lat=lat, beam=beam, coords=coords, aperture=0.05, turns=args.turns or STEP_TURNS)
     lat, beam = W.dba_ring(), W.dba_beam()
     coords = W.dba_particles(args.n_gauss, args.grid, seed=rank)
     return dict(name=(f"DBA ring, 20 cells + RF (401 elements), 3 GeV e-, {args.n_gauss:,} Gaussian + "
                       f"{args.grid}x{args.grid} DA grid, aperture 0.02 m"),
-                lat=lat, beam=beam, coords=coords, aperture=0.02, turns=STEP_TURNS)
+                lat=lat, beam=beam, coords=coords, aperture=0.02, turns=args.turns or STEP_TURNS)
+
+
+def batched_workload(args, rank, time_dependent=False):
+    import trackpad_b200.workloads as W
+    if time_dependent:
+        nvar = args.nvar or 64
+        turns = args.turns or 50
+        run_turns = 500  # the ramp and the modulation are defined over the full 500-turn run
+        variants = [(W.time_dependent(v, run_turns), 16384)
+                    for v, _ in W.dba_variants(nvar=nvar, seed=11 + rank, n_base=16384)]
+        name = (f"{nvar} time-dependent DBA variants (4..20 cells, strengths +-2%, Q1 k1 ramp +1% over 500 turns, "
+                f"RF voltage 5% at a 200-turn period), 16,384 Gaussian particles each, aperture 0.02 m")
+    else:
+        nvar = args.nvar or 256
+        turns = args.turns or 100
+        variants = W.dba_variants(nvar=nvar, seed=1 + rank, n_base=4096)
+        name = (f"{nvar} DBA variants (4..20 cells, strengths +-2%), 4,096 x U[0.25, 1] Gaussian particles each, "
+                f"aperture 0.02 m, one CUDA-graph launch")
+    counts = [n for _, n in variants]
+    poff = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    coords = np.asfortranarray(np.concatenate([W.gaussian(n, seed=1000 * rank + i) for i, n in enumerate(counts)]))
+    return dict(name=name, lats=[v for v, _ in variants], counts=counts, poff=poff, coords=coords,
+                beam=W.dba_beam(), aperture=0.02, turns=turns)
 
 
 def cpu_baseline(w, target_s=10.0, chunk=1024, threads=0):
@@ -121,19 +165,20 @@ def cpu_baseline(w, target_s=10.0, chunk=1024, threads=0):
     nthreads = threads or oracle_ref.lib().orc_max_threads()
     n = w["coords"].shape[0]
     rng = np.random.Generator(np.random.Philox(1234))
+    turns = min(w["turns"], STEP_TURNS)
     units, dt, chunks = 0.0, 0.0, 0
     while dt < target_s and chunks < 4096:
         idx = rng.integers(0, n, chunk)
         c = np.asfortranarray(w["coords"][idx])
         lost = np.zeros(len(c), np.int64)
         t0 = time.perf_counter()
-        oracle_ref.ringpass(lat, c, lost, tp.beti(beam), w["turns"], aperture=w["aperture"], nthreads=nthreads)
+        oracle_ref.ringpass(lat, c, lost, tp.beti(beam), turns, aperture=w["aperture"], nthreads=nthreads)
         dt += time.perf_counter() - t0
-        units += float(len(c)) * len(lat) * w["turns"]
+        units += float(len(c)) * len(lat) * turns
         chunks += 1
     return {"value": units / dt, "unit": "particle*element*turns/s", "cores": nthreads, "kind": "port",
-            "sample": f"{chunks} x {chunk} particles drawn from the workload's beam, {w['turns']} turns each "
-                      f"(one step), OpenMP over particles, {dt:.1f} s"}
+            "sample": f"{chunks} x {chunk} particles drawn from the workload's beam, {turns} turns each, "
+                      f"OpenMP over particles, {dt:.1f} s"}
 
 
 def run_reference(args):
@@ -164,26 +209,51 @@ def run_reference(args):
     print(json.dumps(line))
 
 
-# DRAM bytes per particle of one tracking launch: ncu capture of track_single on
-# the DBA ring, 69,632 particles x 10 turns (5.425 MB read + written).  Traffic
-# grows with the particle count (the table lives in shared memory).
-DRAM_BYTES_PER_PARTICLE = 5.425152e6 / 69632
-
-
-def main():
-    args = parse()
-    if args.impl == "reference":
-        return run_reference(args)
-    rank, world, local = dist_env()
+# ---------------------------------------------------------------------------
+# Adjoint / forward ratio on the gradient workload
+# ---------------------------------------------------------------------------
+def adjoint_ratio(tp, local, turns=256, n=65536, warmup=1, steps=1):
+    """Loss and gradient with respect to the 120 quadrupole k1 and 80 sextupole
+    k2 of the DBA ring, 65,536 Gaussian particles, `turns` turns, against
+    ringpass! of the same beam; device times from the library's CUDA events."""
     import torch
-    import __graft_entry__
-    tp = __graft_entry__.load_package()
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    import trackpad_b200.workloads as W
+    lat, beam = W.dba_ring(), W.dba_beam()
+    params = W.magnet_indices(lat)
+    dev = torch.device("cuda", local)
+    init = torch.from_numpy(np.ascontiguousarray(W.gaussian(n, seed=0).T)).to(dev)
+    coords = torch.empty_like(init)
+    lost = torch.zeros(n, dtype=torch.int64, device=dev)
+    fwd, adj, rev, st = [], [], [], None
+    loss = None
+    for i in range(warmup + steps):
+        coords.copy_(init)
+        lost.zero_()
+        tp.ringpass_(coords.T, lat, beam, lost, turns, aperture=0.02)
+        f = tp.last_stats(local)["kernel_ms"]
+        loss, _ = tp.ringpass_adjoint(init.T, lat, beam, None, turns, params, sigma=SIGMA_LOSS,
+                                      lost_weight=LOST_WEIGHT, aperture=0.02)
+        st = tp.adjoint_stats()
+        if i >= warmup:
+            fwd.append(f)
+            adj.append(st["forward_ms"] + st["reverse_ms"])
+            rev.append(st["reverse_ms"])
+    f, a = float(np.median(fwd)), float(np.median(adj))
+    return {"metric": "adjoint/forward time ratio", "value": a / f, "unit": "x", "higher_is_better": False,
+            "config": f"DBA ring (401 elements), {n:,} Gaussian particles, {turns} turns, gradient w.r.t. "
+                      f"{sum(1 for e in params if lat.elements[e].kind == 'QUADRUPOLE')} k1 + "
+                      f"{sum(1 for e in params if lat.elements[e].kind == 'SEXTUPOLE')} k2, loss = mean "
+                      f"(x^2+y^2)/sigma^2 + 1e3 lost fraction, sigma = 1e-4 m",
+            "forward_ms": f, "adjoint_ms": a, "adjoint_forward_pass_ms": a - float(np.median(rev)),
+            "adjoint_reverse_ms": float(np.median(rev)), "checkpoint_every": st["checkpoint_every"],
+            "checkpoint_bytes": st["checkpoint_bytes"], "reconstruction_error": st["reconstruction_error"],
+            "loss": loss, "target": "<= 3"}
+
+
+# ---------------------------------------------------------------------------
+# Single-lattice tracking (default)
+# ---------------------------------------------------------------------------
+def main_track(args, tp, torch, rank, world, local, dist):
     w = workload(args, rank)
     lat, beam, aperture, turns = w["lat"], w["beam"], w["aperture"], w["turns"]
     n = w["coords"].shape[0]
@@ -271,6 +341,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(w)
+    adj = None
+    if args.workload == "dba" and world == 1 and not args.no_adjoint:
+        adj = adjoint_ratio(tp, local)
 
     if rank == 0:
         line = {
@@ -289,7 +362,225 @@ def main():
                          "flops_per_launch": flops / args.steps, "kernel_ms": k_ms},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
         }
+        if adj is not None:
+            line["adjoint"] = adj
         print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# Batched forward tracking
+# ---------------------------------------------------------------------------
+def main_batched(args, tp, torch, rank, world, local, dist):
+    w = batched_workload(args, rank)
+    dev = torch.device("cuda", local)
+    n = w["coords"].shape[0]
+    batch = tp.Batch(w["lats"], device=local)
+    betis = np.full(len(w["lats"]), tp.beti(w["beam"]))
+    init = torch.from_numpy(np.ascontiguousarray(w["coords"].T)).to(dev)
+    coords = torch.empty_like(init)
+    lost = torch.zeros(n, dtype=torch.int64, device=dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+    turns = w["turns"]
+
+    def step():
+        coords.copy_(init)
+        lost.zero_()
+        batch.ringpass_(coords.T, w["poff"], betis, lost, turns, aperture=w["aperture"], use_graph=True,
+                        stream=sptr)
+        st = tp.last_stats(local)
+        flush.fill_(1)
+        return st
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = Clocks(local)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    kernel_ms, flops, units, launches = [], 0.0, 0.0, 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        st = step()
+        kernel_ms.append(st["kernel_ms"])
+        flops += st["flops"]
+        units += st["units"]
+        launches += st["launches"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    elapsed = e0.elapsed_time(e1) / 1e3
+    t = torch.tensor([elapsed, units], dtype=torch.float64, device=dev)
+    if dist:
+        dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
+        dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
+    elapsed, units_all = float(t[0]), float(t[1])
+    peak = tp.probe_fp64_peak(local)
+    k_ms = float(np.mean(kernel_ms))
+    achieved = (flops / args.steps) / (k_ms * 1e-3) / 1e12
+
+    # The plain tracker run lattice by lattice on the same beams (a sample of
+    # variants, same turns): what batching replaces.
+    lbl = None
+    if rank == 0:
+        nsample = min(16, len(w["lats"]))
+        u, tms = 0.0, 0.0
+        for v in range(nsample):
+            s = slice(int(w["poff"][v]), int(w["poff"][v + 1]))
+            c = init[:, s].contiguous()
+            l = torch.zeros(c.shape[1], dtype=torch.int64, device=dev)
+            for rep in range(2):
+                c.copy_(init[:, s])
+                l.zero_()
+                tp.ringpass_(c.T, w["lats"][v], w["beam"], l, turns, aperture=w["aperture"], stream=sptr)
+                stv = tp.last_stats(local)
+            u += stv["units"]
+            tms += stv["kernel_ms"]
+        lbl = {"value": u / (tms * 1e-3), "unit": "particle*element*turns/s",
+               "sample": f"the first {nsample} variants, one ringpass! launch each, device time"}
+
+    e2e = None
+    if not args.no_e2e:
+        hbuf = torch.empty((6, n), dtype=torch.float64).pin_memory()
+        hl = torch.empty(n, dtype=torch.int64).pin_memory().numpy()
+        hc = hbuf.numpy().T
+        e2e_units, t_e2e = 0.0, 0.0
+        for i in range(3):
+            hc[...] = w["coords"]
+            hl[...] = 0
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            batch.ringpass_(hc, w["poff"], betis, hl, turns, aperture=w["aperture"], use_graph=True)
+            t1 = time.perf_counter()
+            stt = tp.last_stats(local)
+            if i > 0:
+                t_e2e += t1 - t0
+                e2e_units += stt["units"]
+        e2e = {"value": e2e_units / t_e2e * world, "unit": "particle*element*turns/s",
+               "h2d_bytes_per_step": int(stt["h2d_bytes"]), "d2h_bytes_per_step": int(stt["d2h_bytes"])}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(dict(lat=w["lats"][0], beam=w["beam"], coords=w["coords"][:w["counts"][0]],
+                                aperture=w["aperture"], turns=turns))
+        cpu["sample"] = "variant 0: " + cpu["sample"]
+    if rank == 0:
+        line = {
+            "metric": "particle*element*turns/s FP64", "value": units_all / elapsed,
+            "unit": "particle*element*turns/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox variants and Gaussian beams)",
+            "config": {"workload": w["name"], "turns_per_step": turns, "particles_per_gpu": n,
+                       "variants": len(w["lats"]), "elements": [int(min(len(x) for x in w["lats"])),
+                                                                int(max(len(x) for x in w["lats"]))],
+                       "l2": "flushed between timed steps (256 MiB write)",
+                       "fp": "no FMA contraction (reference operation order)"},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": DRAM_BYTES_PER_PARTICLE * n,
+                         "traffic_source": "per-particle DRAM bytes of the single-lattice capture, scaled",
+                         "peak_source": "measured FP64 FMA throughput of this device (tp_probe_fp64_peak)",
+                         "flops_per_launch": flops / args.steps, "kernel_ms": k_ms},
+            "lattice_by_lattice": lbl, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+        }
+        print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# Gradients
+# ---------------------------------------------------------------------------
+def main_adjoint(args, tp, torch, rank, world, local, dist):
+    import trackpad_b200.workloads as W
+    turns = args.turns or 256
+    clocks = Clocks(local)
+    r = adjoint_ratio(tp, local, turns=turns, warmup=max(1, min(args.warmup, 2)), steps=args.steps)
+    clk = clocks.stop()
+    # end to end through the public API with host arrays (inputs staged every call)
+    lat, beam = W.dba_ring(), W.dba_beam()
+    c0 = W.gaussian(65536, seed=0)
+    params = W.magnet_indices(lat)
+    t0 = time.perf_counter()
+    tp.ringpass_adjoint(c0, lat, beam, None, turns, params, sigma=SIGMA_LOSS, lost_weight=LOST_WEIGHT, aperture=0.02)
+    t_adj = time.perf_counter() - t0
+    c = c0.copy(order="F")
+    l = np.zeros(len(c), np.int64)
+    t0 = time.perf_counter()
+    tp.ringpass_(c, lat, beam, l, turns, aperture=0.02)
+    t_fwd = time.perf_counter() - t0
+    if rank == 0:
+        line = {"metric": r["metric"], "value": r["value"], "unit": "x", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["adjoint_ms"], "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox beam)",
+                "config": {"workload": r["config"]}, "detail": r,
+                "e2e": {"value": t_adj / t_fwd, "unit": "x", "h2d_bytes_per_step": 65536 * 48,
+                        "d2h_bytes_per_step": 8 * (1 + len(params))},
+                "gpu_launches": 3 * args.steps, "clocks": clk}
+        print(json.dumps(line))
+
+
+def main_batched_adjoint(args, tp, torch, rank, world, local, dist):
+    w = batched_workload(args, rank, time_dependent=True)
+    import trackpad_b200.workloads as W
+    dev = torch.device("cuda", local)
+    n = w["coords"].shape[0]
+    batch = tp.Batch(w["lats"], device=local)
+    betis = np.full(len(w["lats"]), tp.beti(w["beam"]))
+    params = [W.magnet_indices(l) for l in w["lats"]]
+    init = torch.from_numpy(np.ascontiguousarray(w["coords"].T)).to(dev)
+    coords = torch.empty_like(init)
+    lost = torch.zeros(n, dtype=torch.int64, device=dev)
+    turns = w["turns"]
+    stream = torch.cuda.current_stream(dev)
+    clocks = Clocks(local)
+    fwd, adj, rev = [], [], []
+    for i in range(max(1, min(args.warmup, 2)) + args.steps):
+        coords.copy_(init)
+        lost.zero_()
+        batch.ringpass_(coords.T, w["poff"], betis, lost, turns, aperture=w["aperture"], use_graph=True,
+                        stream=stream.cuda_stream)
+        f = tp.last_stats(local)["kernel_ms"]
+        loss, grads = batch.ringpass_adjoint(init.T, w["poff"], betis, None, turns, params, sigma=SIGMA_LOSS,
+                                             lost_weight=LOST_WEIGHT, aperture=w["aperture"])
+        st = tp.adjoint_stats()
+        if i >= max(1, min(args.warmup, 2)):
+            fwd.append(f)
+            adj.append(st["forward_ms"] + st["reverse_ms"])
+            rev.append(st["reverse_ms"])
+    clk = clocks.stop()
+    f, a = float(np.median(fwd)), float(np.median(adj))
+    if rank == 0:
+        line = {"metric": "adjoint/forward time ratio", "value": a / f, "unit": "x", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": a, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (seeded Philox variants and beams)",
+                "config": {"workload": w["name"], "turns_per_step": turns,
+                           "parameters": int(sum(len(p) for p in params))},
+                "detail": {"batched_forward_ms": f, "batched_adjoint_ms": a, "reverse_ms": float(np.median(rev)),
+                           "checkpoint_every": st["checkpoint_every"], "checkpoint_bytes": st["checkpoint_bytes"],
+                           "reconstruction_error": st["reconstruction_error"],
+                           "forward_rate": st["units"] / (f * 1e-3), "target": "<= 3"},
+                "gpu_launches": 3 * args.steps, "clocks": clk}
+        print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    rank, world, local = dist_env()
+    import torch
+    import __graft_entry__
+    tp = __graft_entry__.load_package()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    fn = {"dba": main_track, "fodo": main_track, "batched": main_batched, "adjoint": main_adjoint,
+          "batched_adjoint": main_batched_adjoint}[args.workload]
+    fn(args, tp, torch, rank, world, local, dist)
     if dist:
         dist.barrier()
         dist.destroy_process_group()

@@ -216,6 +216,42 @@ def test_batched_adjoint_equals_lattice_by_lattice():
         assert np.array_equal(grads[i], g1)
 
 
+def test_batched_time_dependent_adjoint():
+    """The time-dependent batched adjoint workload at small size: per-variant
+    loss and gradient equal the single-lattice adjoint, and the dual-number
+    oracle for one variant."""
+    variants = W.dba_variants(nvar=3, seed=8, n_base=120, cells_range=(2, 3))
+    nt = 12
+    lats = [W.time_dependent(v, nt) for v, _ in variants]
+    batch = tp.Batch(lats)
+    beam = W.dba_beam()
+    counts = [n for _, n in variants]
+    poff = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    coords = np.asfortranarray(np.concatenate([W.gaussian(n, seed=50 + i) for i, n in enumerate(counts)]))
+    params = [W.magnet_indices(v) for v, _ in variants]
+    loss, grads = batch.ringpass_adjoint(coords, poff, np.full(len(counts), tp.beti(beam)), None, nt, params,
+                                         sigma=SIGMA, aperture=0.02, checkpoint_every=5)
+    for i, lat in enumerate(lats):
+        c = np.asfortranarray(coords[poff[i]:poff[i + 1]])
+        l1, g1 = tp.ringpass_adjoint(c, lat, beam, None, nt, params[i], sigma=SIGMA, aperture=0.02,
+                                     checkpoint_every=5)
+        assert loss[i] == l1 and np.array_equal(grads[i], g1)
+    # variant 0 against the oracle with the same per-turn values
+    base, _ = variants[0]
+    td = lats[0]
+    fields, cols = [], []
+    for j, e in enumerate(td.elements):
+        if isinstance(e, tp.TimeVaryingElement):
+            for name in e.updates:
+                fields += [j, 1 if name == "k1" else 5]
+                cols.append([float(e.updates[name](tp.TimeContext(0.0, t))) for t in range(nt)])
+    vals = np.array(cols).T
+    c0 = np.asfortranarray(coords[:counts[0]])
+    rloss, rg, _ = oracle_grad(base, c0, beam, nt, params[0], 0.02, sched=(fields, 0, vals))
+    assert abs(loss[0] - rloss) <= 1e-12 * abs(rloss)
+    assert_grad_close(grads[0], rg)
+
+
 def test_tangent_maps_match_oracle_and_are_symplectic():
     lat, beam = W.dba_ring(cells=2), W.dba_beam()
     orbits = np.concatenate([np.zeros((1, 6)), W.gaussian(7, seed=31)])

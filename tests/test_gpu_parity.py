@@ -98,6 +98,7 @@ def test_fodo_ring_cpu_workload():
     coords = W.gaussian(10000, seed=0)
     _, lost, st = _compare(lat, beam, coords, 100, 0.05, 1e-10)
     assert st["particles"] == 10000 and st["units"] == 10000 * 32 * 100
+    assert st["element_passes"] == int((lost == 0).sum()) * 32 * 100 or lost.any()
 
 
 @pytest.mark.parametrize("contract", [False, True])
@@ -121,6 +122,14 @@ def test_dba_ten_turns_with_losses():
     c, lost, st = _compare(lat, beam, coords, 10, 0.02, 1e-11, regular=regular, rtol_other=1e-6)
     assert 0 < lost.sum() < len(lost)
     assert st["survivors"] == int((lost == 0).sum())
+    # maps evaluated: every turn of a survivor, and up to the element of loss of a lost particle
+    c2 = coords.copy(order="F")
+    l2 = np.zeros(len(c2), np.int64)
+    lt = np.full(len(c2), -1, np.int32)
+    le = np.full(len(c2), -1, np.int32)
+    tp.ringpass_(c2, lat, beam, l2, 10, aperture=0.02, lost_turn=lt, lost_elem=le)
+    expect = int((l2 == 0).sum()) * len(lat) * 10 + int((lt[l2 == 1].astype(np.int64) * len(lat) + le[l2 == 1] + 1).sum())
+    assert tp.last_stats()["element_passes"] == expect
 
 
 @pytest.mark.parametrize("schedule", [1, 2])
@@ -252,6 +261,30 @@ def test_batched_equals_lattice_by_lattice():
             rc = np.asfortranarray(ref[s])
             rl = np.zeros(n, np.int64)
             tp.ringpass_(rc, lat, beam, rl, 4, aperture=0.02, schedule=1)
+            assert np.array_equal(c[s], rc) and np.array_equal(l[s], rl)
+
+
+def test_batched_time_dependent_equals_lattice_by_lattice():
+    """Variants with a ramped quadrupole family and a modulated RF voltage in one
+    batched launch == each variant on its own; a new turn range rebuilds the
+    batch's per-turn tables (and its CUDA graph)."""
+    variants = W.dba_variants(nvar=3, seed=7, n_base=150, cells_range=(2, 3))
+    lats = [W.time_dependent(v, 40) for v, _ in variants]
+    batch = tp.Batch(lats)
+    beam = W.dba_beam()
+    counts = [n for _, n in variants]
+    poff = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    coords = np.asfortranarray(np.concatenate([W.gaussian(n, seed=40 + i) for i, n in enumerate(counts)]))
+    for turn0, use_graph in ((2, True), (2, True), (9, True), (9, False)):
+        c = coords.copy(order="F")
+        l = np.zeros(len(c), np.int64)
+        batch.ringpass_(c, poff, np.full(len(counts), tp.beti(beam)), l, 6, turn=turn0, aperture=0.02,
+                        use_graph=use_graph)
+        for i, lat in enumerate(lats):
+            s = slice(poff[i], poff[i + 1])
+            rc = np.asfortranarray(coords[s])
+            rl = np.zeros(counts[i], np.int64)
+            tp.ringpass_(rc, lat, beam, rl, 6, turn=turn0, aperture=0.02, schedule=1)
             assert np.array_equal(c[s], rc) and np.array_equal(l[s], rl)
 
 

@@ -41,7 +41,7 @@ struct TrackArgs {
     int32_t exact;              // exact Hamiltonian drift
     int32_t refill;             // lane-refill scheduling
     unsigned long long* work;   // refill counter (scratch, zeroed by the host)
-    unsigned long long* passes; // particle-element maps evaluated (scratch, zeroed)
+    unsigned long long* passes; // unused by the kernels (element passes are derived from the loss records)
     int32_t* err;               // device error word (scratch, zeroed)
     // Batched (ragged) launches: variant v owns particles [poff[v], poff[v+1])
     // and program words [toff[v], toff[v+1]).  nvar == 0 for single lattices.

@@ -20,6 +20,9 @@
 //   d asin(px/d2) = (dpx - px*dd2/d2) / pz.
 // The bend_fringe coefficients are differentiated in forward mode with a
 // three-direction dual number (px, py, dp1), the only inputs they have.
+// Inside a K-turn segment the rebuilt states drift from the forward ones by
+// the rounding of the inverse maps (about 1e-13 absolute per turn on the DBA
+// ring); each segment restarts from its stored state.
 #pragma once
 #include "tp_maps.cuh"
 
@@ -379,6 +382,39 @@ __device__ __forceinline__ double fringe_phi(double px, double py, double dp1, d
     return -b0 * libm::tan(b0 * gK * term1 * pz - libm::atan(term2));
 }
 
+// The coefficients with gK = 0 (no fringe-field integral: the case of the
+// reference's ERBend defaults).  Then tan(-atan(u)) = -u gives
+// phi = b0 xp / (1 + yp^2), and 1/cos^2(atan(u)) = 1 + u^2 with
+// u = px pz / (py^2 + pz^2), so no transcendental function is left.
+__device__ __forceinline__ void fringe_coeffs_gk0(D3 px, D3 py, D3 dp1, double b0, D3& phi, D3& dpx, D3& dpy,
+                                                  D3& dd) {
+    D3 px2 = px * px;
+    D3 py2 = py * py;
+    D3 pz2 = dp1 * dp1 - px2 - py2;
+    D3 pz = d3_sqrt(pz2);
+    D3 ipz = d3(1.0) / pz;
+    D3 xp = px * ipz;
+    D3 yp = py * ipz;
+    phi = b0 * (xp / (1.0 + yp * yp));
+    D3 pz4 = pz2 * pz2;
+    D3 py2z2 = py2 + pz2;
+    D3 u = px * pz / py2z2;
+    D3 powsec = 1.0 + u * u;
+    D3 denom = pz4 * pz * (py2 * py2 + px2 * pz2 + 2.0 * py2 * pz2 + pz4);
+    D3 w = powsec / denom;
+    D3 a = px * pz4;
+    dpx = (-b0) * ((px2 * pz4 * (py2 - pz2) - pz4 * pz2 * py2z2) * w);
+    dpy = (-b0) * (py * a * py2z2 * w);
+    dd = b0 * (dp1 * a * (py2 - pz2) * w);
+}
+
+__device__ __forceinline__ double fringe_phi_gk0(double px, double py, double dp1, double b0) {
+    double pz = pxyz(dp1 * dp1, px, py);
+    double xp = px / pz;
+    double yp = py / pz;
+    return b0 * (xp / (1.0 + yp * yp));
+}
+
 // bend_fringe, Forest 13.13 (:752-815): with yf the new y,
 //   x' = x + dpx yf^2/2, y' = yf, py' = py - phi yf, z' = z - dd yf^2/2,
 // where yf = 2y / (1 + sqrt(1 - 2 dpy y)) solves y = yf - dpy yf^2 / 2, and
@@ -389,13 +425,24 @@ __device__ __noinline__ void rev_bend_fringe(P6& r, L6& l, double b0, double gK,
     const double dp1v = beti + r.d;
     const double yf = r.y;
     double py = r.py;
-    for (int it = 0; it < 12; ++it) {
-        const double pn = r.py + fringe_phi(r.px, py, dp1v, b0, gK) * yf;
-        if (pn == py) break;
-        py = pn;
-    }
     D3 phi, dpx, dpy, dd;
-    fringe_coeffs(D3{r.px, 1.0, 0.0, 0.0}, D3{py, 0.0, 1.0, 0.0}, D3{dp1v, 0.0, 0.0, 1.0}, b0, gK, phi, dpx, dpy, dd);
+    if (gK == 0.0) {
+        for (int it = 0; it < 12; ++it) {
+            const double pn = r.py + fringe_phi_gk0(r.px, py, dp1v, b0) * yf;
+            if (pn == py) break;
+            py = pn;
+        }
+        fringe_coeffs_gk0(D3{r.px, 1.0, 0.0, 0.0}, D3{py, 0.0, 1.0, 0.0}, D3{dp1v, 0.0, 0.0, 1.0}, b0, phi, dpx, dpy,
+                          dd);
+    } else {
+        for (int it = 0; it < 12; ++it) {
+            const double pn = r.py + fringe_phi(r.px, py, dp1v, b0, gK) * yf;
+            if (pn == py) break;
+            py = pn;
+        }
+        fringe_coeffs(D3{r.px, 1.0, 0.0, 0.0}, D3{py, 0.0, 1.0, 0.0}, D3{dp1v, 0.0, 0.0, 1.0}, b0, gK, phi, dpx, dpy,
+                      dd);
+    }
     const double yf2 = yf * yf;
     r.x = r.x - 0.5 * dpx.v * yf2;
     r.y = yf - 0.5 * dpy.v * yf2;
@@ -418,58 +465,81 @@ __device__ __noinline__ void rev_bend_fringe(P6& r, L6& l, double b0, double gK,
     l.d = l.d + ldp1;
 }
 
-// exact_bend_body, Forest 12.18 (:858-894), one call of length L backwards.
-// cs, sn = cos, sin(irho L).  The inverse is the same body with -L.
-__device__ __forceinline__ void rev_body_one(P6& r, L6& l, double h, double L, double Lbeti, double cs, double sn,
-                                             double beti, bool straight) {
-    const double dp1 = beti + r.d;
-    const double D = dp1 * dp1;
-    if (straight) {
-        // exact drift with pz = sqrt(dp1^2 - px^2 - py^2)
-        const double pz2 = D - r.px * r.px - r.py * r.py;
-        const double pz = pz2 > 0.0 ? sqrt(pz2) : 0.0;
-        const double N = L / pz;
-        r.x = r.x - r.px * N;
-        r.y = r.y - r.py * N;
-        r.z = r.z - N * dp1 + Lbeti;
-        const double g = l.x * r.px + l.y * r.py + l.z * dp1;
-        const double q = g * N / pz2;
-        l.px = l.px + l.x * N + q * r.px;
-        l.py = l.py + l.y * N + q * r.py;
-        l.d = l.d + l.z * N - q * dp1;
-        return;
-    }
-    // Inverse: body(-L) on the output; its pz is the forward pz' and its
-    // pxyz(px_new) is the forward pz.
+// exact_bend_body, Forest 12.18 (:858-894), backwards.  cs, sn = cos, sin(irho L).
+// The inverse is the same body with -L: on the output (px', py, delta) it
+// computes pz' = pxyz(px') and the forward's asin(px'/d2), then the input px,
+// its pz and asin(px/d2).  py and delta are unchanged by the body, so d2 is
+// fixed, and in a run of bodies without kicks between them the input values of
+// one reversed call are the output values of the next one reversed: they are
+// carried (RevBody), leaving one asin, one sqrt and one division per call.
+struct RevBody {
+    double D, d2, id2, ih, pzo, ipzo, aso;
+};
+
+__device__ __forceinline__ void rev_body_init(const P6& r, double h, double dp1, RevBody& c) {
+    c.D = dp1 * dp1;
+    c.d2 = pxyz(c.D, 0.0, r.py);
+    c.id2 = 1.0 / c.d2;
+    c.ih = 1.0 / h;
+    c.pzo = pxyz(c.D, r.px, r.py);
+    c.ipzo = 1.0 / c.pzo;
+    c.aso = libm::asin(jclamp(r.px * c.id2));
+}
+
+__device__ __forceinline__ void rev_body_step(P6& r, L6& l, RevBody& c, double h, double L, double Lbeti, double cs,
+                                              double sn, double dp1) {
     const double pxo = r.px;  // forward output px'
-    const double pzo = pxyz(D, pxo, r.py);
-    const double pzmxo = pzo - (1.0 + r.x * h);
+    const double pzmxo = c.pzo - (1.0 + r.x * h);
     const double px = pxo * cs - pzmxo * sn;
-    const double d2 = pxyz(D, 0.0, r.py);
-    const double id2 = 1.0 / d2;
-    const double ih = 1.0 / h;
-    const double das = libm::asin(jclamp(px * id2)) - libm::asin(jclamp(pxo * id2));  // as1 - as2 of the forward
-    const double dasin = L + das * ih;                                                  // forward dasin
-    const double pz = pxyz(D, px, r.py);
-    const double x = (pz - pzmxo * cs - pxo * sn - 1.0) * ih;
-    r.x = x;
+    const double asi = libm::asin(jclamp(px * c.id2));
+    const double dasin = L + (asi - c.aso) * c.ih;  // forward dasin
+    const double pz = pxyz(c.D, px, r.py);
+    const double ipz = 1.0 / pz;
+    r.x = (pz - pzmxo * cs - pxo * sn - 1.0) * c.ih;
     r.px = px;
     r.y = r.y - r.py * dasin;
     r.z = r.z - dp1 * dasin + Lbeti;
     // cotangents at the rebuilt input
-    const double ipz = 1.0 / pz, ipzo = 1.0 / pzo;
-    const double lds = (l.y * r.py + l.z * dp1) * ih;  // cotangent of (as1 - as2)
-    const double lpzo = l.x * ih;
-    const double lpxn = l.px - lds * ipzo - lpzo * pxo * ipzo;
-    const double lpzmx = -l.x * cs * ih + lpxn * sn;
-    const double lpz = lpzmx;
-    const double lx = -h * lpzmx;
-    const double lpx = l.x * sn * ih + lds * ipz + lpxn * cs - lpz * px * ipz;
-    const double ld2 = lds * id2 * (pxo * ipzo - px * ipz);
-    const double lD = 0.5 * (lpzo * ipzo + ld2 * id2 + lpz * ipz);
-    const double lpy = l.py + l.y * dasin - (lpzo * ipzo + ld2 * id2 + lpz * ipz) * r.py;
-    const double ld = l.d + l.z * dasin + 2.0 * dp1 * lD;
-    l.x = lx; l.px = lpx; l.py = lpy; l.d = ld;
+    const double lds = (l.y * r.py + l.z * dp1) * c.ih;  // cotangent of (as1 - as2)
+    const double lpzo = l.x * c.ih;
+    const double lpxn = l.px - (lds + lpzo * pxo) * c.ipzo;
+    const double lpzmx = -l.x * cs * c.ih + lpxn * sn;
+    const double lpx = l.x * sn * c.ih + (lds - lpzmx * px) * ipz + lpxn * cs;
+    const double ld2 = lds * c.id2 * (pxo * c.ipzo - px * ipz);
+    const double sq = lpzo * c.ipzo + ld2 * c.id2 + lpzmx * ipz;  // 2 x cotangent of D
+    const double lpy = l.py + l.y * dasin - sq * r.py;
+    const double ld = l.d + l.z * dasin + dp1 * sq;
+    l.x = -h * lpzmx; l.px = lpx; l.py = lpy; l.d = ld;
+    c.pzo = pz;
+    c.ipzo = ipz;
+    c.aso = asi;
+}
+
+// Straight body (|irho| < 1e-6): an exact drift with pz = sqrt(dp1^2 - px^2 - py^2).
+__device__ __forceinline__ void rev_body_straight(P6& r, L6& l, double L, double Lbeti, double dp1) {
+    const double pz2 = dp1 * dp1 - r.px * r.px - r.py * r.py;
+    const double pz = pz2 > 0.0 ? sqrt(pz2) : 0.0;
+    const double N = L / pz;
+    r.x = r.x - r.px * N;
+    r.y = r.y - r.py * N;
+    r.z = r.z - N * dp1 + Lbeti;
+    const double g = l.x * r.px + l.y * r.py + l.z * dp1;
+    const double q = g * N / pz2;
+    l.px = l.px + l.x * N + q * r.px;
+    l.py = l.py + l.y * N + q * r.py;
+    l.d = l.d + l.z * N - q * dp1;
+}
+
+__device__ __forceinline__ void rev_body_one(P6& r, L6& l, double h, double L, double Lbeti, double cs, double sn,
+                                             double beti, bool straight) {
+    const double dp1 = beti + r.d;
+    if (straight) {
+        rev_body_straight(r, l, L, Lbeti, dp1);
+        return;
+    }
+    RevBody c;
+    rev_body_init(r, h, dp1, c);
+    rev_body_step(r, l, c, h, L, Lbeti, cs, sn, dp1);
 }
 
 template <int M>
@@ -484,11 +554,14 @@ __device__ __noinline__ void rev_exact_body(P6& r, L6& l, const double* w, const
     const double L1b = L1 * beti, L2b = L2 * beti;
     const double cs1 = w[eb::CS1], sn1 = w[eb::SN1], cs2 = w[eb::CS2], sn2 = w[eb::SN2];
     if ((h.flags & RF_NOKICK) && !straight) {
+        const double dp1 = beti + r.d;
+        RevBody c;
+        rev_body_init(r, irho, dp1, c);
 #pragma unroll 1
         for (int k = 4 * h.nsteps - 1; k >= 0; --k) {
             const bool outer = ((k & 3) == 0) || ((k & 3) == 3);
-            rev_body_one(r, l, irho, outer ? L1 : L2, outer ? L1b : L2b, outer ? cs1 : cs2, outer ? sn1 : sn2, beti,
-                         false);
+            rev_body_step(r, l, c, irho, outer ? L1 : L2, outer ? L1b : L2b, outer ? cs1 : cs2, outer ? sn1 : sn2,
+                          dp1);
         }
         return;
     }

@@ -166,8 +166,9 @@ __global__ void k_alive_mask(const int64_t* lost, int64_t n, uint8_t* alive0, un
 __global__ void k_work_stats(const uint8_t* alive0, const int64_t* lost, const int32_t* lost_turn,
                              const int32_t* lost_elem, int64_t n, const double* prefix, const int64_t* poff,
                              const int64_t* pref_off, const int32_t* nelem_v, int32_t nvar, int32_t nelem, int32_t nturns,
-                             int32_t turn0, unsigned long long* survivors, double* flops) {
-    unsigned long long surv = 0;
+                             int32_t turn0, unsigned long long* survivors, double* flops,
+                             unsigned long long* passes) {
+    unsigned long long surv = 0, ps = 0;
     double f = 0.0, u = 0.0;
     for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) {
         if (!alive0[i]) continue;
@@ -187,17 +188,22 @@ __global__ void k_work_stats(const uint8_t* alive0, const int64_t* lost, const i
         if (lost[i] != 1) {
             surv += 1;
             f += double(nturns) * per_turn;
+            ps += (unsigned long long)nturns * (unsigned long long)ne;
         } else {
             int full = lost_turn[i] - turn0;
             f += double(full) * per_turn + (lost_elem[i] >= 0 && ne > 0 ? pre[lost_elem[i]] : 0.0);
+            // the maps evaluated: full turns, then the elements up to and including the one of loss
+            ps += (unsigned long long)full * (unsigned long long)ne + (unsigned long long)(lost_elem[i] + 1);
         }
     }
     for (int o = 16; o > 0; o >>= 1) {
+        ps += __shfl_down_sync(0xffffffffu, ps, o);
         surv += __shfl_down_sync(0xffffffffu, surv, o);
         f += __shfl_down_sync(0xffffffffu, f, o);
         u += __shfl_down_sync(0xffffffffu, u, o);
     }
     if ((threadIdx.x & 31) == 0) {
+        if (ps) atomicAdd(passes, ps);
         if (surv) atomicAdd(survivors, surv);
         if (f != 0.0) atomicAdd(flops, f);
         if (u != 0.0) atomicAdd(flops + 1, u);
@@ -689,7 +695,7 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     if (le != 0) return cuda_err(cudaError_t(le), "track kernel launch");
     TP_CUDA(cudaEventRecord(c->ev1, s));
     k_work_stats<<<sg, 256, 0, s>>>(c->alive0, d_lost, d_lt, d_le, n, prefix, nullptr, nullptr, nullptr, 0, a.nelem,
-                                     nturns, turn0, c->counters + 3, c->flops_acc);
+                                     nturns, turn0, c->counters + 3, c->flops_acc, c->counters + 1);
     TP_CUDA(cudaGetLastError());
     if (!dev) {
         TP_CUDA(cudaMemcpyAsync(coords, d_coords, size_t(n) * 6 * sizeof(double), cudaMemcpyDeviceToHost, s));
@@ -1005,7 +1011,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
         if (le != 0) return cuda_err(cudaError_t(le), "batched track kernel launch");
         if (timed) TP_CUDA(cudaEventRecord(c->ev1, q));
         k_work_stats<<<sg, 256, 0, q>>>(c->alive0, d_lost, d_lt, d_le, n, d_pre, b->poff, d_pre_off, b->nelem_v, nvar,
-                                        0, nturns, turn0, c->counters + 3, c->flops_acc);
+                                        0, nturns, turn0, c->counters + 3, c->flops_acc, c->counters + 1);
         TP_CUDA(cudaGetLastError());
         return TP_OK;
     };

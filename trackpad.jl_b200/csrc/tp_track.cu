@@ -130,8 +130,7 @@ __device__ __forceinline__ const double* resolve(const double* rec, RecHdr& h, c
 // (`nelem` records).  Slot state is per lane.  With REFILL, lanes take new
 // particles from `next_particle` at turn boundaries until it returns < 0.
 template <bool EXACT, bool REFILL, typename NextFn>
-__device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, double beti, NextFn next_particle,
-                         unsigned long long& passes) {
+__device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, double beti, NextFn next_particle) {
     const double beta = 1.0 / beti;
     const double beta2 = beta * beta;
     const int lane = threadIdx.x & 31;
@@ -166,9 +165,10 @@ __device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, doubl
         for (int e = 0; e < nelem; ++e) {
             RecHdr h0 = *reinterpret_cast<const RecHdr*>(rec);
             const double* next = rec + h0.words;
-            unsigned live = __ballot_sync(0xffffffffu, act);
-            if (live == 0) break;  // every lane of this warp is empty: skip the rest of the turn
-            if (lane == 0) passes += __popc(live);
+            // Every lane of this warp empty: skip the rest of the turn.  (The vote
+            // at every element also reconverges the warp after divergent maps;
+            // voting every 16 elements measured 4% slower on the DBA ring.)
+            if (__ballot_sync(0xffffffffu, act) == 0) break;
             if (act) {
                 RecHdr h = h0;
                 const double* r = resolve(rec, h, a, a.turn0 + t);
@@ -217,7 +217,6 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_single(TrackAr
         }
         tab = smem;
     }
-    unsigned long long passes = 0;
     if (REFILL) {
         auto next = [&](unsigned need, int lane, bool& more) -> int64_t {
             unsigned long long base = 0;
@@ -229,16 +228,15 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_single(TrackAr
             unsigned long long j = base + __popc(need & ((1u << lane) - 1u));
             return j < (unsigned long long)a.n ? int64_t(j) : -1;
         };
-        run_warp<EXACT, true>(a, tab, a.nelem, a.beti, next, passes);
+        run_warp<EXACT, true>(a, tab, a.nelem, a.beti, next);
     } else {
         const int64_t gid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
         auto next = [&](unsigned need, int lane, bool& more) -> int64_t {
             more = false;
             return gid < a.n ? gid : -1;
         };
-        run_warp<EXACT, false>(a, tab, a.nelem, a.beti, next, passes);
+        run_warp<EXACT, false>(a, tab, a.nelem, a.beti, next);
     }
-    if ((threadIdx.x & 31) == 0 && passes) atomicAdd(a.passes, passes);
 }
 
 // Batched: warps take 32-particle tiles (variant, first particle) in variant
@@ -246,7 +244,6 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_single(TrackAr
 template <bool EXACT>
 __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_batched(TrackArgs a, const int64_t* tile_off) {
     const int lane = threadIdx.x & 31;
-    unsigned long long passes = 0;
     const int64_t ntiles = tile_off[a.nvar];
     for (;;) {
         unsigned long long tile = 0;
@@ -274,12 +271,11 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_batched(TrackA
             av.sched_stride = int32_t(a.sched_v[4 * v + 1]);
             av.sched_turn0 = int32_t(a.sched_v[4 * v + 2]);
             av.sched_nturns = int32_t(a.sched_v[4 * v + 3]);
-            run_warp<EXACT, false>(av, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next, passes);
+            run_warp<EXACT, false>(av, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next);
         } else {
-            run_warp<EXACT, false>(a, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next, passes);
+            run_warp<EXACT, false>(a, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next);
         }
     }
-    if (lane == 0 && passes) atomicAdd(a.passes, passes);
 }
 
 static size_t smem_bytes(const TrackArgs& a) { return size_t(a.smem_words) * 8; }

@@ -41,6 +41,10 @@ struct TpOpts
     aperture_x::Float64; aperture_y::Float64; stream::Ptr{Cvoid}
 end
 
+struct TpLossSpec
+    kind::Int32; reserved::Int32; sigma::Float64; lost_weight::Float64
+end
+
 const TP_KIND = Dict{DataType,Int32}(
     Marker => 0, Drift => 1, Quadrupole => 2, Sextupole => 3, Octupole => 4, ThinMultipole => 5,
     SBend => 6, ExactSBend => 7, RFCavity => 8, Solenoid => 9, Corrector => 10, Translation => 11,
@@ -96,7 +100,7 @@ mutable struct DeviceLattice
     handle::Ptr{Cvoid}
 end
 
-function DeviceLattice(lat::Lattice)
+function DeviceLattice(lat::Lattice; strengths = nothing)
     elems = TpElem[]; mis = TpMisalign[]
     for e in lat.elements
         b = e isa TimeVaryingElement ? e.base : e
@@ -106,6 +110,13 @@ function DeviceLattice(lat::Lattice)
             idx = Int32(length(mis) - 1)
         end
         push!(elems, pack(b, idx))
+    end
+    if strengths !== nothing  # (element indices, values): the main strength k of those records
+        for (i, k) in zip(strengths...)
+            r = elems[i]
+            elems[i] = TpElem(ntuple(j -> fieldname(TpElem, j) === :k ? Float64(k) : getfield(r, j),
+                                     fieldcount(TpElem))...)
+        end
     end
     h = Ref{Ptr{Cvoid}}(C_NULL)
     GC.@preserve elems mis begin
@@ -192,6 +203,69 @@ function TrackPad.ringpass!(::B200, coords::Matrix{Float64}, lat::Lattice, beam:
                     time, dt_turn, turn, o), "tp_ringpass")
     end
     nothing
+end
+
+# --- Derivatives ---------------------------------------------------------------
+"""
+    loss_and_gradient(coords0, lat, beam, nturns, params; sigma, lost_weight = 1e3, ks = nothing, ...)
+
+Loss of the tracked beam, mean over survivors of (x^2 + y^2)/sigma^2 plus
+lost_weight x lost fraction, and its gradient with respect to the strength
+(k1, k2, k3) of the Quadrupole/Sextupole/Octupole elements `params` (1-based
+indices into `lat.elements`), from the B200 adjoint (tp_ringpass_adjoint).
+`ks`, if given, replaces those strengths.  coords0 is read only.
+"""
+function loss_and_gradient(coords0::Matrix{Float64}, lat::Lattice, beam::Beam{Float64}, nturns::Int,
+                           params::AbstractVector{<:Integer}; sigma::Real, lost_weight::Real = 1e3, ks = nothing,
+                           aperture::Real = 0.0, time::Real = 0.0, dt_turn::Real = 0.0, turn::Integer = 0,
+                           checkpoint_every::Integer = 0)
+    size(coords0, 2) == 6 || throw(ArgumentError("coords0 must be N x 6"))
+    d = DeviceLattice(lat; strengths = ks === nothing ? nothing : (params, ks))
+    set_schedule!(d, lat, time, dt_turn, turn, max(nturns, 1))
+    p0 = Int32[i - 1 for i in params]
+    loss = Ref(0.0); grad = zeros(length(params))
+    spec = Ref(TpLossSpec(0, 0, Float64(sigma), Float64(lost_weight)))
+    o = Ref(opts(false; aperture = Float64(aperture)))
+    GC.@preserve coords0 p0 grad begin
+        check(ccall((:tp_ringpass_adjoint, LIB), Cint,
+                    (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}, Int64, Ptr{Int64}, Float64, Int32, Float64, Float64,
+                     Int32, Ptr{Int32}, Int32, Ref{TpLossSpec}, Int32, Ref{Float64}, Ptr{Float64}, Ptr{Float64},
+                     Ptr{Int64}, Ref{TpOpts}),
+                    context(), d.handle, coords0, size(coords0, 1), C_NULL, beti(beam), nturns, time, dt_turn, turn,
+                    p0, length(p0), spec, checkpoint_every, loss, grad, C_NULL, C_NULL, o), "tp_ringpass_adjoint")
+    end
+    loss[], grad
+end
+
+"""beam_loss(ks, coords0, lat, beam, nturns, params; sigma, ...): the loss alone,
+differentiable in `ks` (ChainRulesCore rrule and Enzyme reverse rule in
+TrackPadB200ADExt)."""
+beam_loss(ks, coords0, lat, beam, nturns, params; kw...) =
+    loss_and_gradient(coords0, lat, beam, nturns, params; ks = ks, kw...)[1]
+# Positional form (sigma, lost_weight) for the Enzyme rule, whose arguments are annotated one by one.
+beam_loss(ks, coords0, lat, beam, nturns, params, sigma::Real, lost_weight::Real) =
+    loss_and_gradient(coords0, lat, beam, nturns, params; ks = ks, sigma = sigma, lost_weight = lost_weight)[1]
+
+"""
+    tangent_maps(lat, beam, orbits; nturns = 1) -> (M, err)
+
+Exact tangent maps of `nturns` passes about each row of `orbits` (n x 6) and
+their symplecticity error ||M'JM - J||, J = diag(J2, J2, -J2): the device
+counterpart of one_turn_map (src/optics.jl:110-121, finite differences there).
+"""
+function tangent_maps(lat::Lattice, beam::Beam{Float64}, orbits::Matrix{Float64}; nturns::Int = 1, turn::Integer = 0)
+    d = DeviceLattice(lat)
+    set_schedule!(d, lat, 0.0, 0.0, turn, max(nturns, 1))
+    n = size(orbits, 1)
+    jac = zeros(36, n); err = zeros(n)
+    o = Ref(opts(false))
+    GC.@preserve orbits jac err begin
+        check(ccall((:tp_one_turn_jacobian, LIB), Cint,
+                    (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}, Int64, Float64, Int32, Int32, Ptr{Float64}, Ptr{Float64},
+                     Ref{TpOpts}),
+                    context(), d.handle, orbits, n, beti(beam), nturns, turn, jac, err, o), "tp_one_turn_jacobian")
+    end
+    [reshape(jac[:, i], 6, 6) for i in 1:n], err
 end
 
 end # module

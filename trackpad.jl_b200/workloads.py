@@ -3,6 +3,8 @@
   fodo_ring()      FODO ring on 1 GeV electrons: QF(0.5 m, +1.2) D(2.0) QD(0.5 m, -1.2) D(2.0), 8 cells.
   dba_ring()       DBA storage ring on 3 GeV electrons: 20 cells of 25 m, 401 elements with the RF cavity.
   dba_variants()   ragged batch of DBA rings (4..20 cells, strengths perturbed by U[-2%, 2%]).
+  time_dependent() a lattice whose Q1 quadrupole family ramps k1 linearly by +1% over a run and whose RF
+                   voltage is modulated by 5% with a 200-turn period (the time-dependent adjoint workload).
   gaussian()       seeded 6D Gaussian beam in the reference's N x 6 column-major layout.
   da_grid()        dynamic-aperture grid of (x, y) amplitudes, other coordinates zero.
 
@@ -14,7 +16,7 @@ import math
 import numpy as np
 
 from .elements import C_LIGHT, Drift, ExactSBend, Quadrupole, RFCavity, Sextupole
-from .tracking import Beam, Lattice
+from .tracking import Beam, Lattice, timed
 
 SIGMA = (1e-4, 1e-5, 1e-4, 1e-5, 1e-3, 1e-4)  # x, px, y, py, z, delta
 
@@ -105,6 +107,21 @@ def dba_variants(nvar=256, seed=1, n_base=4096, perturb=0.02, cells_range=(4, 20
         npart = int(round(n_base * rng.uniform(0.25, 1.0)))
         out.append((dba_ring(cells, strengths), npart))
     return out
+
+
+def time_dependent(lat, nturns, family="Q1", ramp=0.01, rf_depth=0.05, rf_period=200.0):
+    """`lat` with k1 of every quadrupole named `family` ramped linearly by
+    `ramp` (relative) over `nturns` turns, and the RF voltage modulated by
+    `rf_depth` with a period of `rf_period` turns: per-turn field functions
+    (timed / Turn(), src/time_dependence.jl:46, 147-155)."""
+    elems = list(lat.elements)
+    for i, e in enumerate(elems):
+        if e.kind == "QUADRUPOLE" and e.name == family:
+            elems[i] = timed(e, k1=lambda ctx, k0=e.k1: k0 * (1.0 + ramp * ctx.turn / nturns))
+        elif e.kind == "RFCAVITY":
+            elems[i] = timed(e, volt=lambda ctx, v0=e.volt: v0 * (1.0 + rf_depth *
+                                                                 math.sin(2.0 * math.pi * ctx.turn / rf_period)))
+    return Lattice(elems, name=lat.name + "_TD")
 
 
 def gaussian(n, seed=0, sigma=SIGMA):
