@@ -475,6 +475,8 @@ def main_batched(args, tp, torch, rank, world, local, dist):
             "config": {"workload": w["name"], "turns_per_step": turns, "particles_per_gpu": n,
                        "variants": len(w["lats"]), "elements": [int(min(len(x) for x in w["lats"])),
                                                                 int(max(len(x) for x in w["lats"]))],
+                       "schedule": {1: "static tiles", 2: "pooled refill"}.get(st["schedule"], st["schedule"]),
+                       "survivors": st["survivors"],
                        "l2": "flushed between timed steps (256 MiB write)",
                        "fp": "no FMA contraction (reference operation order)"},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

@@ -160,7 +160,11 @@ typedef struct tp_opts {
                                   bends amplify a changed rounding to ~1e-11)     */
     int32_t block_size;        /* threads per block; 0 = autotuned                */
     int32_t ppt;               /* particles per thread (1 or 2); 0 = autotuned    */
-    int32_t schedule;          /* 0 = autotuned, 1 = static, 2 = lane refill      */
+    int32_t schedule;          /* 0 = autotuned: the first two multi-turn calls of a
+                                  configuration run static and lane refill, later
+                                  calls the faster (all give identical results);
+                                  1 = static, 2 = lane refill (batched: lanes of a
+                                  variant refill from that variant's particles)   */
     int32_t reserved0;
     double aperture_x;         /* rectangular aperture half widths [m]; a value   */
     double aperture_y;         /* <= 0 disables it (reference limits remain)      */

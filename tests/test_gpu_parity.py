@@ -264,6 +264,54 @@ def test_batched_equals_lattice_by_lattice():
             assert np.array_equal(c[s], rc) and np.array_equal(l[s], rl)
 
 
+@pytest.mark.parametrize("schedule", [1, 2])
+def test_batched_schedules_with_losses_equal_lattice_by_lattice(schedule):
+    """Static tiles and pooled refill (lanes of a variant refilled from that
+    variant's particles after losses) give the same bits as each variant alone."""
+    variants = W.dba_variants(nvar=5, seed=4, n_base=200, cells_range=(2, 5))
+    batch = tp.Batch([v for v, _ in variants])
+    beam = W.dba_beam()
+    counts = [n for _, n in variants]
+    poff = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    coords = np.asfortranarray(np.concatenate([np.concatenate([W.gaussian(n // 2, seed=60 + i),
+                                                               W.da_grid(1, n - n // 2, half=0.019)])
+                                               for i, n in enumerate(counts)]))
+    c = coords.copy(order="F")
+    l = np.zeros(len(c), np.int64)
+    lt = np.full(len(c), -1, np.int32)
+    le = np.full(len(c), -1, np.int32)
+    batch.ringpass_(c, poff, np.full(len(counts), tp.beti(beam)), l, 12, aperture=0.02, lost_turn=lt, lost_elem=le,
+                    schedule=schedule, use_graph=False)
+    assert tp.last_stats()["schedule"] == schedule
+    assert 0 < l.sum() < len(l)
+    for i, (lat, n) in enumerate(variants):
+        s = slice(poff[i], poff[i + 1])
+        rc = np.asfortranarray(coords[s])
+        rl = np.zeros(n, np.int64)
+        rlt = np.full(n, -1, np.int32)
+        rle = np.full(n, -1, np.int32)
+        tp.ringpass_(rc, lat, beam, rl, 12, aperture=0.02, lost_turn=rlt, lost_elem=rle, schedule=1)
+        assert np.array_equal(c[s], rc) and np.array_equal(l[s], rl)
+        assert np.array_equal(lt[s], rlt) and np.array_equal(le[s], rle)
+
+
+def test_autotuned_schedule_settles_and_keeps_results():
+    """schedule=0: the first two multi-turn calls try static and refill, later
+    calls keep one of them; every call gives the same bits."""
+    lat, beam = W.dba_ring(cells=2), W.dba_beam()
+    c0 = np.asfortranarray(np.concatenate([W.gaussian(300, seed=70), W.da_grid(16, 16)]))
+    seen, outs = [], []
+    for _ in range(4):
+        c = c0.copy(order="F")
+        l = np.zeros(len(c), np.int64)
+        tp.ringpass_(c, lat, beam, l, 6, aperture=0.02)
+        seen.append(tp.last_stats()["schedule"])
+        outs.append((c, l))
+    assert seen[:2] == [1, 2] and seen[2] == seen[3] and seen[2] in (1, 2)
+    for c, l in outs[1:]:
+        assert np.array_equal(c, outs[0][0]) and np.array_equal(l, outs[0][1])
+
+
 def test_batched_time_dependent_equals_lattice_by_lattice():
     """Variants with a ramped quadrupole family and a modulated RF voltage in one
     batched launch == each variant on its own; a new turn range rebuilds the

@@ -50,6 +50,7 @@ struct TrackArgs {
     const double* beti_v;
     const int32_t* nelem_v;
     const int64_t* sched_v;     // batched: per variant word offset into `sched` (-1: none), stride, first turn, turns
+    unsigned long long* pool;   // batched with refill: per variant count of particles handed out (zeroed)
     int32_t nvar;
     int32_t smem_words;         // words staged into shared memory per block
 };

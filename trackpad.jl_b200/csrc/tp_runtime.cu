@@ -11,6 +11,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <initializer_list>
 #include <mutex>
 #include <new>
 #include <string>
@@ -42,6 +43,43 @@ int cuda_err(cudaError_t e, const char* where) {
 
 constexpr int kMaxDevices = 16;
 
+// Online choice of the particle scheduling (1 = static, 2 = lane refill).
+// Every schedule gives bit-identical results, so the first two calls of a
+// configuration (same sizes, turns, drift and build) run one schedule each on
+// the caller's own work, timed with the call's CUDA events, and later calls
+// keep the faster one.
+struct SchedTune {
+    uint64_t key = 0;
+    int trials = 0;
+    float ms[2] = {0.f, 0.f};
+    int best = 1;
+};
+
+uint64_t tune_key(std::initializer_list<int64_t> parts) {
+    uint64_t h = 1469598103934665603ull;  // FNV-1a over the parts
+    for (int64_t v : parts) {
+        for (int k = 0; k < 8; ++k) {
+            h ^= uint64_t(v >> (8 * k)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    }
+    return h | 1ull;
+}
+
+int tune_pick(SchedTune& t, uint64_t key) {
+    if (t.key != key) {
+        t = SchedTune{};
+        t.key = key;
+    }
+    return t.trials < 2 ? 1 + t.trials : t.best;
+}
+
+void tune_record(SchedTune& t, uint64_t key, int schedule, float ms) {
+    if (t.key != key || t.trials >= 2 || schedule != 1 + t.trials) return;
+    t.ms[schedule - 1] = ms;
+    if (++t.trials == 2) t.best = t.ms[1] < t.ms[0] ? 2 : 1;
+}
+
 // Device copy of a lattice on one device.
 struct DevLattice {
     double* table = nullptr;
@@ -50,6 +88,7 @@ struct DevLattice {
     double* prefix = nullptr;  // inclusive prefix sums of per-element flops
     size_t sched_bytes = 0;
     uint64_t version = 0;
+    SchedTune tune;
 };
 
 }  // namespace
@@ -93,11 +132,13 @@ struct tp_batch {
     double* sched = nullptr;           // concatenated per-turn schedule tables
     int64_t* sched_v = nullptr;        // per variant: word offset (-1: none), stride, first turn, turns
     std::vector<uint64_t> h_ver;       // lattice versions the device tables were built from
+    unsigned long long* pool = nullptr; // per variant particles handed out (pooled refill)
+    SchedTune tune;
     std::vector<int64_t> h_sched_v;
     // cached CUDA graph of the launch sequence
     cudaGraphExec_t graph = nullptr;
     std::vector<int64_t> g_poff;
-    int32_t g_nturns = -1, g_turn0 = 0, g_exact = -1, g_strict = -1;
+    int32_t g_nturns = -1, g_turn0 = 0, g_exact = -1, g_strict = -1, g_refill = -1;
     double g_limx = 0, g_limy = 0;
     const void* g_coords = nullptr;
     const void* g_lost = nullptr;
@@ -668,13 +709,27 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     const size_t table_bytes = L->program.size() * sizeof(double);
     const size_t smem = table_bytes + 64 <= c->smem_optin ? table_bytes : 0;
     a.smem_words = smem ? int32_t(L->program.size()) : 0;
-    // Launch configuration: lane refill for multi-turn tracks (loss frees lanes),
-    // static for single passes (short lattices are HBM-bound).
-    int schedule = o.schedule ? o.schedule : (nturns > 1 ? 2 : 1);
-    a.refill = schedule == 2 ? 1 : 0;
+    // Launch configuration: static for single passes; for multi-turn tracks the
+    // schedule the caller asks for, else the tuned one (lane refill frees the
+    // lanes of lost particles, static has less bookkeeping).
     int block = o.block_size > 0 ? o.block_size : 128;
     block = std::max(32, std::min(kTrackMaxBlock, block / 32 * 32));
     const bool strict = o.fp_contract == 0;
+    const uint64_t tkey = tune_key({n, nturns, int64_t(exact), int64_t(strict), block, int64_t(L->version),
+                                    int64_t(L->program.size())});
+    bool tuning = false;
+    int schedule = o.schedule;
+    if (schedule == 0) {
+        if (nturns <= 1) {
+            schedule = 1;
+        } else {
+            std::lock_guard<std::mutex> g(L->mu);
+            SchedTune& tu = L->dev[c->device].tune;
+            schedule = tune_pick(tu, tkey);
+            tuning = tu.trials < 2;
+        }
+    }
+    a.refill = schedule == 2 ? 1 : 0;
     int bps = 0;
     int oerr = strict ? occupancy_track_strict(block, 1, smem, &bps) : occupancy_track_fast(block, 1, smem, &bps);
     if (oerr != 0 || bps <= 0) bps = 1;
@@ -713,6 +768,10 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     if (st != TP_OK) return st;
     float ms = 0.f;
     TP_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    if (tuning) {
+        std::lock_guard<std::mutex> g(L->mu);
+        tune_record(L->dev[c->device].tune, tkey, schedule, ms);
+    }
     tp_stats& S = c->stats;
     S.particles = int64_t(cnt[2]);
     S.survivors = int64_t(cnt[3]);
@@ -757,8 +816,10 @@ TP_API int tp_ringpass(tp_ctx* c, const tp_lattice* L, double* coords, int64_t n
 static void batch_free_tables(tp_batch* b) {
     cudaFree(b->table); cudaFree(b->toff); cudaFree(b->nelem_v); cudaFree(b->beti_v); cudaFree(b->poff);
     cudaFree(b->mis); cudaFree(b->prefix); cudaFree(b->prefix_off); cudaFree(b->sched); cudaFree(b->sched_v);
+    cudaFree(b->pool);
     b->table = nullptr; b->toff = nullptr; b->nelem_v = nullptr; b->beti_v = nullptr; b->poff = nullptr;
     b->mis = nullptr; b->prefix = nullptr; b->prefix_off = nullptr; b->sched = nullptr; b->sched_v = nullptr;
+    b->pool = nullptr;
     if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
 }
 
@@ -833,7 +894,7 @@ static int batch_build(tp_batch* b) {
     pre_e.insert(pre_e.end(), pre_l.begin(), pre_l.end());
     cudaError_t e = cudaMalloc(&b->table, std::max<size_t>(table.size(), 2) * sizeof(double));
     if (e == cudaSuccess) e = cudaMemcpy(b->table, table.data(), table.size() * sizeof(double), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMalloc(&b->toff, 2 * (size_t(nvar) + 1) * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&b->toff, 3 * (size_t(nvar) + 1) * sizeof(int64_t));
     if (e == cudaSuccess) e = cudaMemcpy(b->toff, b->h_toff.data(), (size_t(nvar) + 1) * sizeof(int64_t), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMalloc(&b->nelem_v, size_t(nvar) * sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMemcpy(b->nelem_v, b->h_nelem.data(), size_t(nvar) * sizeof(int32_t), cudaMemcpyHostToDevice);
@@ -852,6 +913,7 @@ static int batch_build(tp_batch* b) {
         e = cudaMalloc(&b->sched, sched.size() * sizeof(double));
         if (e == cudaSuccess) e = cudaMemcpy(b->sched, sched.data(), sched.size() * sizeof(double), cudaMemcpyHostToDevice);
     }
+    if (e == cudaSuccess) e = cudaMalloc(&b->pool, size_t(nvar) * sizeof(unsigned long long));
     if (e == cudaSuccess) e = cudaMalloc(&b->sched_v, b->h_sched_v.size() * sizeof(int64_t));
     if (e == cudaSuccess)
         e = cudaMemcpy(b->sched_v, b->h_sched_v.data(), b->h_sched_v.size() * sizeof(int64_t), cudaMemcpyHostToDevice);
@@ -947,12 +1009,22 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
         if (lost_turn) { TP_CUDA(cudaMemcpyAsync(d_lt, lost_turn, size_t(n) * 4, cudaMemcpyHostToDevice, s)); h2d += n * 4; }
         if (lost_elem) { TP_CUDA(cudaMemcpyAsync(d_le, lost_elem, size_t(n) * 4, cudaMemcpyHostToDevice, s)); h2d += n * 4; }
     }
-    // Per-variant offsets, betas, tile offsets and flop prefix tables.
-    std::vector<int64_t> offs(2 * (size_t(nvar) + 1));
+    // Per-variant offsets, betas, tile offsets and flop prefix tables.  Tiles
+    // are handed out longest first: the variants with the most elements (the
+    // longest 32-particle loads) come first, so that short loads fill the end
+    // of the launch.  Layout: toff[nvar+1], tile offsets in that order
+    // [nvar+1], the order itself [nvar].
+    std::vector<int32_t> order(static_cast<size_t>(nvar));
+    for (int32_t v = 0; v < nvar; ++v) order[size_t(v)] = v;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t x, int32_t y) { return b->h_nelem[size_t(x)] > b->h_nelem[size_t(y)]; });
+    std::vector<int64_t> offs(3 * (size_t(nvar) + 1));
     for (int32_t v = 0; v <= nvar; ++v) offs[size_t(v)] = b->h_toff[size_t(v)];
     int64_t tiles = 0;
-    for (int32_t v = 0; v < nvar; ++v) {
-        offs[size_t(nvar) + 1 + size_t(v)] = tiles;
+    for (int32_t k = 0; k < nvar; ++k) {
+        const int32_t v = order[size_t(k)];
+        offs[size_t(nvar) + 1 + size_t(k)] = tiles;
+        offs[2 * (size_t(nvar) + 1) + size_t(k)] = v;
         tiles += (poff[v + 1] - poff[v] + 31) / 32;
     }
     offs[2 * (size_t(nvar) + 1) - 1] = tiles;
@@ -987,7 +1059,23 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     a.nvar = nvar;
     a.sched = b->sched;
     a.sched_v = b->sched_v;
+    a.pool = b->pool;
     int block = o.block_size > 0 ? std::max(32, std::min(kTrackMaxBlock, o.block_size / 32 * 32)) : 128;
+    // Static tiles or pooled refill: the caller's choice, else tuned online.
+    int64_t ph = 0;
+    for (int32_t v = 0; v <= nvar; ++v) ph = ph * 1000003 + poff[v];
+    const uint64_t tkey = tune_key({n, nturns, int64_t(exact), int64_t(strict), block, ph, int64_t(b->table_words)});
+    bool tuning = false;
+    int schedule = o.schedule;
+    if (schedule == 0) {
+        if (nturns <= 1) {
+            schedule = 1;
+        } else {
+            schedule = tune_pick(b->tune, tkey);
+            tuning = b->tune.trials < 2;
+        }
+    }
+    a.refill = schedule == 2 ? 1 : 0;
     int bps = 0;
     int oerr = strict ? occupancy_track_strict(block, 1, 0, &bps) : occupancy_track_fast(block, 1, 0, &bps);
     if (oerr != 0 || bps <= 0) bps = 1;
@@ -1002,6 +1090,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
         TP_CUDA(cudaMemsetAsync(c->counters, 0, 8 * sizeof(unsigned long long), q));
         TP_CUDA(cudaMemsetAsync(c->err, 0, 4 * sizeof(int32_t), q));
         TP_CUDA(cudaMemsetAsync(c->flops_acc, 0, 2 * sizeof(double), q));
+        if (a.refill) TP_CUDA(cudaMemsetAsync(b->pool, 0, size_t(nvar) * sizeof(unsigned long long), q));
         if (!(dev && lost_turn)) k_fill_i32<<<sg, 256, 0, q>>>(d_lt, n, -1);
         if (!(dev && lost_elem)) k_fill_i32<<<sg, 256, 0, q>>>(d_le, n, -1);
         k_alive_mask<<<sg, 256, 0, q>>>(d_lost, n, c->alive0, c->counters + 2);
@@ -1020,6 +1109,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
         bool same = b->graph && b->g_nturns == nturns && b->g_turn0 == turn0 && b->g_exact == int(exact) &&
                     b->g_strict == int(strict) && b->g_limx == a.limx && b->g_limy == a.limy &&
                     b->g_coords == d_coords && b->g_lost == d_lost && b->g_table == b->table &&
+                    b->g_refill == a.refill &&
                     b->g_poff == std::vector<int64_t>(poff, poff + nvar + 1);
         if (!same) {
             if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
@@ -1039,6 +1129,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
             b->g_nturns = nturns; b->g_turn0 = turn0; b->g_exact = int(exact); b->g_strict = int(strict);
             b->g_limx = a.limx; b->g_limy = a.limy; b->g_coords = d_coords; b->g_lost = d_lost;
             b->g_table = b->table;
+            b->g_refill = a.refill;
             b->g_poff.assign(poff, poff + nvar + 1);
         }
         TP_CUDA(cudaEventRecord(c->ev0, s));
@@ -1064,6 +1155,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     if (st != TP_OK) return st;
     float ms = 0.f;
     TP_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    if (tuning) tune_record(b->tune, tkey, schedule, ms);
     tp_stats& S = c->stats;
     S.particles = int64_t(cnt[2]);
     S.survivors = int64_t(cnt[3]);
@@ -1078,7 +1170,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     S.ppt = 1;
     S.grid = grid;
     S.launches = 3 + ((dev && lost_turn) ? 0 : 1) + ((dev && lost_elem) ? 0 : 1);
-    S.schedule = 3;
+    S.schedule = schedule;
     S.fp_contract = strict ? 0 : 1;
     return TP_OK;
 }

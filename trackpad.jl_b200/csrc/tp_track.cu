@@ -239,9 +239,16 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_single(TrackAr
     }
 }
 
-// Batched: warps take 32-particle tiles (variant, first particle) in variant
-// order; tile t of variant v covers particles poff[v] + 32*(t - tile_off[v]).
-template <bool EXACT>
+// Batched: warps take 32-particle tiles (variant, first particle) in the
+// host's hand-out order (variants with the most elements first); tile t of the
+// k-th variant v = order[k] covers particles poff[v] + 32*(t - tile_off[k]).
+// Static (REFILL false): the warp tracks exactly its tile's particles.  Pooled
+// refill (REFILL true): a warp that takes a tile of variant v draws particles
+// of v from the variant's pool counter (pool[v], zeroed by the host) and
+// refills lanes freed by a loss at turn boundaries until the pool is empty;
+// later tiles of an emptied variant end at once.  Either way every particle is
+// tracked from turn 0 with its own turn counter, so the results are the same.
+template <bool EXACT, bool REFILL>
 __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_batched(TrackArgs a, const int64_t* tile_off) {
     const int lane = threadIdx.x & 31;
     const int64_t ntiles = tile_off[a.nvar];
@@ -250,19 +257,31 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_batched(TrackA
         if (lane == 0) tile = atomicAdd(a.work, 1ull);
         tile = __shfl_sync(0xffffffffu, tile, 0);
         if (tile >= (unsigned long long)ntiles) break;
-        // variant of this tile: last v with tile_off[v] <= tile
+        // position k of this tile's variant in the hand-out order (last k with
+        // tile_off[k] <= tile), and the variant itself
         int lo = 0, hi = a.nvar - 1;
         while (lo < hi) {
             int mid = (lo + hi + 1) >> 1;
             if (tile_off[mid] <= (int64_t)tile) lo = mid; else hi = mid - 1;
         }
-        const int v = lo;
-        const int64_t first = a.poff[v] + 32 * (int64_t(tile) - tile_off[v]);
+        const int v = int(tile_off[a.nvar + 1 + lo]);
+        const int64_t p0 = a.poff[v];
         const int64_t endp = a.poff[v + 1];
-        const int64_t mine = first + lane;
+        const int64_t mine = p0 + 32 * (int64_t(tile) - tile_off[lo]) + lane;
+        const unsigned long long nv = (unsigned long long)(endp - p0);
         auto next = [&](unsigned need, int ln, bool& more) -> int64_t {
-            more = false;
-            return mine < endp ? mine : -1;
+            if (!REFILL) {
+                more = false;
+                return mine < endp ? mine : -1;
+            }
+            unsigned long long base = 0;
+            const int cnt = __popc(need);
+            if (ln == 0) base = atomicAdd(a.pool + v, (unsigned long long)cnt);
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (base + (unsigned long long)cnt >= nv) more = false;
+            if (!((need >> ln) & 1u)) return -1;
+            const unsigned long long j = base + __popc(need & ((1u << ln) - 1u));
+            return j < nv ? p0 + int64_t(j) : -1;
         };
         if (a.sched_v != nullptr && a.sched_v[4 * v] >= 0) {
             // this variant's per-turn schedule
@@ -271,9 +290,9 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_batched(TrackA
             av.sched_stride = int32_t(a.sched_v[4 * v + 1]);
             av.sched_turn0 = int32_t(a.sched_v[4 * v + 2]);
             av.sched_nturns = int32_t(a.sched_v[4 * v + 3]);
-            run_warp<EXACT, false>(av, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next);
+            run_warp<EXACT, REFILL>(av, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next);
         } else {
-            run_warp<EXACT, false>(a, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next);
+            run_warp<EXACT, REFILL>(a, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next);
         }
     }
 }
@@ -284,9 +303,11 @@ int launch(const TrackArgs& a, int grid, int block, int ppt, size_t smem, void* 
     (void)ppt;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (a.nvar > 0) {
-        const int64_t* tile_off = a.toff + (a.nvar + 1);  // host packs tile offsets after toff
-        if (a.exact) track_batched<true><<<grid, block, 0, st>>>(a, tile_off);
-        else track_batched<false><<<grid, block, 0, st>>>(a, tile_off);
+        const int64_t* tile_off = a.toff + (a.nvar + 1);  // host packs tile offsets and the order after toff
+        if (a.exact && a.refill) track_batched<true, true><<<grid, block, 0, st>>>(a, tile_off);
+        else if (a.exact) track_batched<true, false><<<grid, block, 0, st>>>(a, tile_off);
+        else if (a.refill) track_batched<false, true><<<grid, block, 0, st>>>(a, tile_off);
+        else track_batched<false, false><<<grid, block, 0, st>>>(a, tile_off);
         return int(cudaGetLastError());
     }
     (void)smem_bytes;

@@ -413,7 +413,7 @@ class Batch:
 
     def ringpass_(self, coords, poff, betis, lost_flags, nturns, *, time=0.0, dt_turn=0.0, turn=0, aperture=None,
                   lost_turn=None, lost_elem=None, exact=True, contract=False, use_graph=True, block_size=0,
-                  stream=None):
+                  schedule=0, stream=None):
         """ringpass! of every variant in one launch; variant v owns particles
         poff[v]..poff[v+1].  Time-dependent variants are evaluated per turn."""
         b = _Buffers(coords, lost_flags, lost_turn, lost_elem)
@@ -425,7 +425,7 @@ class Batch:
             raise ValueError("poff must have nvar+1 entries and betis nvar entries")
         if poff[-1] != b.n:
             raise ValueError("poff[-1] must equal the number of particles")
-        o = _opts(aperture, exact, contract, b.device, block_size, 0, stream)
+        o = _opts(aperture, exact, contract, b.device, block_size, schedule, stream)
         st = _abi.lib().tp_ringpass_batched(context(self.device), self._handle, b.coords,
                                             poff.ctypes.data_as(C.c_void_p), b.lost, b.lost_turn, b.lost_elem,
                                             betis.ctypes.data_as(C.c_void_p), int(nturns), C.c_double(0.0),
