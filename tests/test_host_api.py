@@ -77,3 +77,17 @@ def test_tracking_rejects_bad_arrays():
         tp.ringpass_(np.zeros((4, 5)), lat, beam, np.zeros(4, np.int64), 1)
     with pytest.raises(TypeError):
         tp.ringpass_(np.zeros((4, 6)), lat, beam, np.zeros(4, np.int32), 1)
+
+
+def test_tune_from_a_known_2x2_map():
+    """twiss_from_2x2 (src/optics.jl:123-149) on R(mu) in Twiss form."""
+    import math
+    for mu, beta, alpha in ((0.3, 12.0, 0.4), (2.0, 3.5, -1.2), (4.5, 7.0, 0.0)):
+        g = (1 + alpha * alpha) / beta
+        M = np.array([[math.cos(mu) + alpha * math.sin(mu), beta * math.sin(mu)],
+                      [-g * math.sin(mu), math.cos(mu) - alpha * math.sin(mu)]])
+        b, a, m, q = tp.optics.twiss_from_2x2(M)
+        assert abs(b - beta) < 1e-12 and abs(a - alpha) < 1e-12
+        assert abs(q - (mu / (2 * math.pi)) % 1.0) < 1e-14
+    with pytest.raises(ValueError):
+        tp.optics.twiss_from_2x2(np.array([[2.0, 1.0], [1.0, 1.0]]))

@@ -403,6 +403,7 @@ double adjoint_stats_time(std::chrono::steady_clock::time_point t0) {
 }
 
 thread_local tp_adjoint_stats g_adj_stats{};
+thread_local int64_t g_last_alive = 0;  // particles alive at the start of the last call
 
 // Build the concatenated device description of `lats`.  params: element
 // indices per variant (param_off[v]..param_off[v+1]), or none (Jacobian).
@@ -649,11 +650,13 @@ int run_adjoint(tp_ctx* c, const std::vector<const tp_lattice*>& lats, const std
     *rec_err = m;
     // particle*element*turns of the forward pass (alive at start x elements x turns)
     double u = 0.0;
+    g_last_alive = 0;
     for (int v = 0; v < nvar; ++v) {
         const int64_t t1 = v + 1 < nvar ? P.var[size_t(v) + 1].tile0 : P.ntiles;
         int64_t a0 = 0;
         for (int64_t t = P.var[size_t(v)].tile0; t < t1; ++t) a0 += cnts[size_t(2 * t)];
         u += double(a0) * double(P.var[size_t(v)].nelem) * double(nturns);
+        g_last_alive += a0;
     }
     *units = u;
     g_adj_stats.checkpoint_every = K;
@@ -768,7 +771,7 @@ TP_API int tp_ringpass_adjoint(tp_ctx* ctx, const tp_lattice* lat, const double*
     }
     tp_stats& S = *ctx_stats(ctx);
     S = tp_stats{};
-    S.particles = n;
+    S.particles = g_last_alive;
     S.survivors = surv;
     S.units = units;
     S.kernel_ms = double(msf) + double(msr);
@@ -837,7 +840,7 @@ TP_API int tp_ringpass_adjoint_batched(tp_ctx* ctx, tp_batch* b, const double* c
     if (pofs[size_t(nvar)] > 0) std::memcpy(grad_out, grad.data(), size_t(pofs[size_t(nvar)]) * 8);
     tp_stats& S = *ctx_stats(ctx);
     S = tp_stats{};
-    S.particles = n;
+    S.particles = g_last_alive;
     for (int64_t x : surv) S.survivors += x;
     S.units = units;
     S.kernel_ms = double(msf) + double(msr);

@@ -1,0 +1,99 @@
+"""Data-parallel tracking over several GPUs, one process per GPU.
+
+Particles are independent, and so are lattice variants, so the tracking path
+shards without any exchange: each rank tracks a contiguous range of the
+particles (one lattice) or a set of whole variants (a batch), on its own GPU.
+The only collective is the adjoint's: the loss and its gradient over the
+union of the ranks' particles need the sums of the per-rank terms, one
+all-reduce of (3 + number of parameters) doubles per gradient.
+
+  particle_shard(n, rank, world)      contiguous [start, stop) of rank's particles
+  variant_shard(costs, world)         variants per rank, balanced by cost (longest first)
+  combine_adjoint(terms, all_reduce)  global loss and gradient from per-rank terms
+  distributed_ringpass_adjoint(...)   the adjoint on this rank's shard, combined over the group
+
+Launch one process per GPU (torchrun); the collective runs on whatever
+process group the caller passes (NCCL for GPU tensors, gloo on CPU).
+"""
+import numpy as np
+
+
+def particle_shard(n, rank, world):
+    """[start, stop) of the particles of `rank` out of `world`: contiguous,
+    sizes differing by at most one."""
+    if world <= 0 or not 0 <= rank < world:
+        raise ValueError("need 0 <= rank < world")
+    base, extra = divmod(int(n), int(world))
+    start = rank * base + min(rank, extra)
+    return start, start + base + (1 if rank < extra else 0)
+
+
+def variant_shard(costs, world):
+    """Assign variants to ranks: longest-processing-time first, each to the
+    rank with the least work so far.  costs[v] is the work of variant v (e.g.
+    elements x particles).  Returns one sorted list of variant indices per rank;
+    the assignment is deterministic, so every rank computes the same one."""
+    costs = [float(c) for c in costs]
+    order = sorted(range(len(costs)), key=lambda v: (-costs[v], v))
+    load = [0.0] * int(world)
+    out = [[] for _ in range(int(world))]
+    for v in order:
+        r = min(range(int(world)), key=lambda k: (load[k], k))
+        out[r].append(v)
+        load[r] += costs[v]
+    return [sorted(x) for x in out]
+
+
+def local_terms(loss, grad, survivors, alive0, lost_weight):
+    """The additive terms of one rank's result: (sum of q over its survivors,
+    survivors, alive at start, survivors x gradient), with
+    loss = sum_q / survivors + lost_weight * (alive0 - survivors) / alive0."""
+    grad = np.asarray(grad, dtype=np.float64)
+    if survivors > 0:
+        frac = (alive0 - survivors) / alive0 if alive0 > 0 else 0.0
+        qsum = (loss - lost_weight * frac) * survivors
+    else:
+        qsum = 0.0
+    return np.concatenate([[qsum, float(survivors), float(alive0)], grad * float(survivors)])
+
+
+def combine_adjoint(terms, all_reduce, lost_weight):
+    """Global (loss, grad) from this rank's `local_terms` vector.  `all_reduce`
+    sums a float64 numpy vector over the ranks in place or returns the sum."""
+    v = np.array(terms, dtype=np.float64)
+    r = all_reduce(v)
+    if r is not None:
+        v = np.asarray(r, dtype=np.float64)
+    qsum, surv, alive = v[0], v[1], v[2]
+    frac = (alive - surv) / alive if alive > 0 else 0.0
+    loss = (qsum / surv if surv > 0 else 0.0) + lost_weight * frac
+    grad = v[3:] / surv if surv > 0 else np.zeros_like(v[3:])
+    return float(loss), grad
+
+
+def torch_all_reduce(group=None, device=None):
+    """A sum all-reduce over a torch.distributed group (NCCL or gloo)."""
+    import torch
+    import torch.distributed as dist
+
+    def reduce(v):
+        t = torch.from_numpy(np.ascontiguousarray(v))
+        if device is not None:
+            t = t.to(device)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        return t.cpu().numpy()
+
+    return reduce
+
+
+def distributed_ringpass_adjoint(coords0, lat, beam, lost0, nturns, params, *, sigma, lost_weight=1e3,
+                                 group=None, device=None, **kw):
+    """Loss and gradient over the particles of every rank of `group`: each rank
+    passes its own shard (`particle_shard`), runs the adjoint on its GPU, and
+    one all-reduce of (3 + len(params)) doubles combines the results."""
+    from . import tracking
+    loss, grad = tracking.ringpass_adjoint(coords0, lat, beam, lost0, nturns, params, sigma=sigma,
+                                           lost_weight=lost_weight, **kw)
+    st = tracking.last_stats()
+    terms = local_terms(loss, grad, st["survivors"], st["particles"], lost_weight)
+    return combine_adjoint(terms, torch_all_reduce(group, device), lost_weight)
