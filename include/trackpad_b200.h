@@ -93,7 +93,14 @@ enum tp_kind {
     TP_OCTUPOLE_SC = 22,    /* OctupoleSC      tracking.jl:1029-1039            */
     TP_SBEND_SC = 23,       /* SBendSC / RBendSC tracking.jl:1041-1070          */
     TP_STRONG_THIN_GAUSSIAN_BEAM = 24, /* tracking.jl:1610-1619                 */
-    TP_KIND_COUNT = 25
+    TP_LBEND = 25,          /* LBend           tracking.jl:1076-1170            */
+    TP_WIGGLER = 26,        /* Wiggler         tracking.jl:1224-1529            */
+    TP_STRONG_GAUSSIAN_BEAM = 27, /* StrongGaussianBeam tracking.jl:1621-1641   */
+    TP_LONGITUDINAL_RLC_WAKE = 28, /* LongitudinalRLCWake tracking.jl:1647-1654,
+                                      elements/wake.jl:27-37                    */
+    TP_LONGITUDINAL_WAKE = 29,     /* LongitudinalWake tracking.jl:1656-1663,
+                                      elements/wake.jl:68-91                    */
+    TP_KIND_COUNT = 30
 };
 
 /* One lattice entry.  Fields use the reference struct field names; a field a
@@ -132,6 +139,21 @@ typedef struct tp_elem {
  *   TP_QUADRUPOLE_SC .. TP_OCTUPOLE_SC  param[0..3] = k0, k1, k2, k3
  *   TP_STRONG_THIN_GAUSSIAN_BEAM  param[0] = amplitude, param[1] = rmssizex,
  *                     param[2] = rmssizey, param[3] = xoffset, param[4] = yoffset
+ *   TP_LBEND          L, angle, e1, e2, fint1, fint2, gap = full_gap,
+ *                     param[0] = K, param[1] = by_error
+ *   TP_LONGITUDINAL_RLC_WAKE  param[0] = freq, param[1] = Rshunt, param[2] = Q0,
+ *                     param[3] = scale
+ * Kinds with array fields read them from the `aux` array of
+ * tp_lattice_create_ex: iparam[0] = word offset of the element's arrays in
+ * aux, iparam[1] = their total length, laid out as
+ *   TP_STRONG_GAUSSIAN_BEAM  aux = zslice_npar[nz], xoffsets[nz], yoffsets[nz]
+ *                     (iparam[1] = 3*nzslice); param[0] = charge,
+ *                     param[1] = total_energy, param[2..3] = beamsize
+ *   TP_LONGITUDINAL_WAKE  aux = times[n], wakefields[n] (iparam[1] = 2n, n >= 2);
+ *                     param[0] = fliphalf, param[1] = scale
+ *   TP_WIGGLER        aux = NHharm, NVharm, rad, By[6*NHharm], Bx[6*NVharm];
+ *                     L, num_int_steps = Nsteps, param[0] = lw, param[1] = Bmax,
+ *                     param[2] = energy
  */
 
 /* Misalignment of one element: entrance translation t1, entrance rotation r1,
@@ -224,6 +246,13 @@ TP_API int tp_beam_beti(double energy, double mass, double* beti_out);
 TP_API int tp_lattice_create(const tp_elem* elems, int64_t n,
                              const tp_misalign* mis, int64_t nmis,
                              tp_lattice** out);
+/* The same with the array fields of StrongGaussianBeam, LongitudinalWake and
+ * Wiggler elements in `aux` (see the per-kind layouts above); the arrays are
+ * copied.  A record may hold at most 65535 words (TP_ERANGE beyond). */
+TP_API int tp_lattice_create_ex(const tp_elem* elems, int64_t n,
+                                const tp_misalign* mis, int64_t nmis,
+                                const double* aux, int64_t naux,
+                                tp_lattice** out);
 TP_API int tp_lattice_destroy(tp_lattice* lat);
 TP_API int tp_lattice_length(const tp_lattice* lat, int64_t* n_out);
 

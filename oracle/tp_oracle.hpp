@@ -50,7 +50,7 @@ constexpr double M_ELECTRON = 0.51099895069e6;
 constexpr double TWO_PI = 6.283185307179586;  // Float64(2pi)
 constexpr double EPS = 2.220446049250313e-16; // eps(Float64)
 
-// Scalar helpers.  sin, cos, tan, asin and atan of a double come from
+// Scalar helpers.  sin, cos, tan, asin, atan, exp, sinh and cosh of a double come from
 // tp_libm.h: the published fdlibm method in explicitly rounded IEEE operations,
 // the implementation the CUDA kernels use, so that the oracle and the device
 // evaluate the same function (both within 1 ulp of the C library).  Other
@@ -62,6 +62,10 @@ inline double cos(double x) { return tp::libm::cos(x); }
 inline double tan(double x) { return tp::libm::tan(x); }
 inline double asin(double x) { return tp::libm::asin(x); }
 inline double atan(double x) { return tp::libm::atan(x); }
+inline double exp(double x) { return tp::libm::exp(x); }
+inline double expm1(double x) { return tp::libm::expm1(x); }
+inline double sinh(double x) { return tp::libm::sinh(x); }
+inline double cosh(double x) { return tp::libm::cosh(x); }
 
 template <class T>
 struct V6 {
@@ -92,11 +96,13 @@ struct Elem {
     T param[8] = {T(0.0), T(0.0), T(0.0), T(0.0), T(0.0), T(0.0), T(0.0), T(0.0)};
     bool has_mis = false, r1nz = false, r2nz = false;
     T t1[6], t2[6], r1[36], r2[36];
+    const double* aux = nullptr;  // the element's array fields (aux + iparam[0]), iparam[1] words
 };
 
 template <class T>
-Elem<T> make_elem(const tp_elem& e, const tp_misalign* mis) {
+Elem<T> make_elem(const tp_elem& e, const tp_misalign* mis, const double* aux = nullptr) {
     Elem<T> o;
+    o.aux = aux ? aux + e.iparam[0] : nullptr;
     o.kind = e.kind;
     o.max_order = e.max_order;
     o.num_int_steps = e.num_int_steps;
@@ -721,7 +727,6 @@ inline V6<T> pass_lorentz(const Elem<T>& e, const V6<T>& r, bool inverse) {
 // StrongThinGaussianBeam: src/tracking.jl:1610-1619
 template <class T>
 inline V6<T> pass_strong_thin_gaussian(const Elem<T>& e, const V6<T>& r) {
-    using std::exp;
     T amp = e.param[0], sx = e.param[1], sy = e.param[2], xo = e.param[3], yo = e.param[4];
     T sx2 = sx * sx;
     if (!(value_of(sx2) >= EPS) && !is_nan(sx2)) sx2 = T(EPS);
@@ -733,6 +738,163 @@ inline V6<T> pass_strong_thin_gaussian(const Elem<T>& e, const V6<T>& r) {
     T px_new = r[1] - g * dx / sx2;
     T py_new = r[3] - g * dy / sy2;
     return V6<T>{{r[0], px_new, r[2], py_new, r[4], r[5]}};
+}
+
+// ---------------------------------------------------------------------------
+// LBend: _lbend_body src/tracking.jl:1076-1150, pass!(::LBend) :1152-1170
+// ---------------------------------------------------------------------------
+template <class T>
+inline V6<T> lbend_body(const V6<T>& r, T L, T grd, T b_angle, T by_error) {
+    using std::abs;
+    using std::sqrt;
+    if (value_of(L) == 0.0) return r;
+    T p_norm = T(1.0) / (T(1.0) + r[5]);
+    T Kx = b_angle / L;
+    T G1 = (Kx * Kx + grd) * p_norm;
+    T G2 = -grd * p_norm;
+    const double tol = 1.4901161193847656e-08;  // sqrt(eps(Float64))
+    T MHD = T(1.0), M12 = L, M21 = T(0.0);
+    T MVD = T(1.0), M34 = L, M43 = T(0.0);
+    T arg1 = T(0.0), arg2 = T(0.0), sqrtG1 = T(0.0), sqrtG2 = T(0.0);
+    if (value_of(abs(G1)) >= tol) {
+        if (value_of(G1) > 0.0) {
+            sqrtG1 = sqrt(G1);
+            arg1 = L * sqrtG1;
+            MHD = cos(arg1); M12 = sin(arg1) / sqrtG1; M21 = -sin(arg1) * sqrtG1;
+        } else {
+            sqrtG1 = sqrt(-G1);
+            arg1 = L * sqrtG1;
+            MHD = cosh(arg1); M12 = sinh(arg1) / sqrtG1; M21 = sinh(arg1) * sqrtG1;
+        }
+    }
+    if (value_of(abs(G2)) >= tol) {
+        if (value_of(G2) > 0.0) {
+            sqrtG2 = sqrt(G2);
+            arg2 = L * sqrtG2;
+            MVD = cos(arg2); M34 = sin(arg2) / sqrtG2; M43 = -sin(arg2) * sqrtG2;
+        } else {
+            sqrtG2 = sqrt(-G2);
+            arg2 = L * sqrtG2;
+            MVD = cosh(arg2); M34 = sinh(arg2) / sqrtG2; M43 = sinh(arg2) * sqrtG2;
+        }
+    }
+    T x = r[0], xpr = r[1] * p_norm, y = r[2], ypr = r[3] * p_norm, delta = r[5];
+    T dterm = delta * p_norm - by_error;
+    T x_new = MHD * x + M12 * xpr;
+    T px_new = (M21 * x + MHD * xpr) / p_norm;
+    if (value_of(abs(G1)) < tol) {
+        x_new = x_new + dterm * L * L * Kx / T(2.0);
+        px_new = px_new + dterm * L * Kx / p_norm;
+    } else if (value_of(G1) > 0.0) {
+        x_new = x_new + dterm * (T(1.0) - cos(arg1)) * Kx / G1;
+        px_new = px_new + dterm * sin(arg1) * Kx / (sqrtG1 * p_norm);
+    } else {
+        x_new = x_new + dterm * (T(1.0) - cosh(arg1)) * Kx / G1;
+        px_new = px_new + dterm * sinh(arg1) * Kx / (sqrtG1 * p_norm);
+    }
+    T y_new = MVD * y + M34 * ypr;
+    T py_new = (M43 * y + MVD * ypr) / p_norm;
+    T z_new = r[4] + xpr * xpr * (L + MHD * M12) / T(4.0);
+    if (value_of(abs(G1)) >= tol) {
+        z_new = z_new + (L - MHD * M12) * (x * x * G1 + dterm * dterm * Kx * Kx / G1 - T(2.0) * x * Kx * dterm) / T(4.0);
+        z_new = z_new + M12 * M21 * (x * xpr - xpr * dterm * Kx / G1) / T(2.0);
+        z_new = z_new + (Kx * x * M12 + xpr * (T(1.0) - MHD) * Kx / G1 + dterm * (L - M12) * Kx * Kx / G1);
+    }
+    z_new = z_new + ((L - MVD * M34) * y * y * G2 + ypr * ypr * (L + MVD * M34)) / T(4.0);
+    z_new = z_new + M34 * M43 * y * ypr / T(2.0);
+    return V6<T>{{x_new, px_new, y_new, py_new, z_new, r[5]}};
+}
+
+template <class T>
+inline V6<T> pass_lbend(const Elem<T>& e, V6<T> r) {
+    r = entrance(e, r);
+    if (value_of(e.L) == 0.0) return nan6<T>();
+    T irho = e.angle / e.L;
+    r = edge_fringe(r, irho, e.e1, e.fint1, e.gap, 1, false);
+    r = lbend_body(r, e.L, e.param[0], e.angle, e.param[1]);
+    r = edge_fringe(r, irho, e.e2, e.fint2, e.gap, 1, true);
+    return exit_(e, r);
+}
+
+// StrongGaussianBeam: src/tracking.jl:1621-1641 (slice arrays in aux)
+template <class T>
+inline V6<T> pass_strong_gaussian(const Elem<T>& e, const V6<T>& r) {
+    using std::abs;
+    const int nz = e.iparam[1] / 3;
+    if (nz <= 0) return r;
+    T bs0 = e.param[2], bs1 = e.param[3];
+    T sx2 = bs0 * bs0;
+    if (!(value_of(sx2) >= EPS) && !is_nan(sx2)) sx2 = T(EPS);
+    T sy2 = bs1 * bs1;
+    if (!(value_of(sy2) >= EPS) && !is_nan(sy2)) sy2 = T(EPS);
+    T ae = abs(e.param[1]);
+    if (!(value_of(ae) >= EPS) && !is_nan(ae)) ae = T(EPS);
+    T factor = e.param[0] / ae;
+    T px = r[1], py = r[3];
+    for (int i = 0; i < nz; ++i) {
+        T w = T(e.aux[i]), xoff = T(e.aux[nz + i]), yoff = T(e.aux[2 * nz + i]);
+        T dx = r[0] - xoff;
+        T dy = r[2] - yoff;
+        T g = w * exp(T(-0.5) * (dx * dx / sx2 + dy * dy / sy2));
+        px = px - factor * g * dx / sx2;
+        py = py - factor * g * dy / sy2;
+    }
+    return V6<T>{{r[0], px, r[2], py, r[4], r[5]}};
+}
+
+// LongitudinalRLCWake: src/tracking.jl:1647-1654, wakefieldfunc_RLCWake
+// src/elements/wake.jl:27-37.  param = freq, Rshunt, Q0, scale.
+template <class T>
+inline V6<T> pass_rlc_wake(const Elem<T>& e, const V6<T>& r) {
+    using std::sqrt;
+    if (value_of(e.param[3]) == 0.0) return r;
+    T zc = r[4] / T(C_LIGHT);
+    T t = is_nan(zc) ? zc : (value_of(zc) > 0.0 ? T(0.0) : zc);  // min(z/c, 0), NaN propagates
+    T Q0 = e.param[2];
+    T Q0p = sqrt(Q0 * Q0 - T(0.25));
+    T w0 = T(TWO_PI) * e.param[0];
+    T w0p = w0 / Q0 * Q0p;
+    T wf;
+    if (value_of(t) > 0.0) {
+        wf = T(0.0);
+    } else {
+        wf = e.param[1] * w0 / Q0 * (cos(w0p * t) + sin(w0p * t) / (T(2.0) * Q0p)) * exp(w0 * t / (T(2.0) * Q0));
+    }
+    return V6<T>{{r[0], r[1], r[2], r[3], r[4], r[5] - e.param[3] * wf}};
+}
+
+// LongitudinalWake: src/tracking.jl:1656-1663, wakefieldfunc and
+// _linear_interpolate src/elements/wake.jl:68-91.  aux = times[n], wakefields[n].
+template <class T>
+inline V6<T> pass_tab_wake(const Elem<T>& e, const V6<T>& r) {
+    if (value_of(e.param[1]) == 0.0) return r;
+    const int n = e.iparam[1] / 2;
+    const double* xs = e.aux;
+    const double* ys = e.aux + n;
+    T t = r[4] / T(C_LIGHT);
+    T wf;
+    if (value_of(t) > xs[0] * value_of(e.param[0])) {
+        wf = T(0.0);
+    } else {
+        T x = t * e.param[0];
+        if (value_of(x) <= xs[0]) {
+            T slope = (T(ys[1]) - T(ys[0])) / (T(xs[1]) - T(xs[0]));
+            wf = T(ys[0]) + slope * (x - T(xs[0]));
+        } else if (value_of(x) >= xs[n - 1]) {
+            T slope = (T(ys[n - 1]) - T(ys[n - 2])) / (T(xs[n - 1]) - T(xs[n - 2]));
+            wf = T(ys[n - 1]) + slope * (x - T(xs[n - 1]));
+        } else {
+            wf = T(ys[n - 1]);
+            for (int i = 1; i < n; ++i) {
+                if (value_of(x) < xs[i]) {
+                    T slope = (T(ys[i]) - T(ys[i - 1])) / (T(xs[i]) - T(xs[i - 1]));
+                    wf = T(ys[i - 1]) + slope * (x - T(xs[i - 1]));
+                    break;
+                }
+            }
+        }
+    }
+    return V6<T>{{r[0], r[1], r[2], r[3], r[4], r[5] - e.param[1] * wf}};
 }
 
 // ---------------------------------------------------------------------------
@@ -764,6 +926,10 @@ inline V6<T> pass(const Elem<T>& e, const V6<T>& r, T beti, bool exact) {
         case TP_SEXTUPOLE_SC: case TP_OCTUPOLE_SC: return pass_multipole_sc(e, r, beti, exact, false);
         case TP_SBEND_SC: return pass_sbend_sc(e, r, beti, exact);
         case TP_STRONG_THIN_GAUSSIAN_BEAM: return pass_strong_thin_gaussian(e, r);
+        case TP_LBEND: return pass_lbend(e, r);
+        case TP_STRONG_GAUSSIAN_BEAM: return pass_strong_gaussian(e, r);
+        case TP_LONGITUDINAL_RLC_WAKE: return pass_rlc_wake(e, r);
+        case TP_LONGITUDINAL_WAKE: return pass_tab_wake(e, r);
         default: return nan6<T>();
     }
 }
@@ -833,6 +999,7 @@ struct Aperture {
 struct Lattice {
     std::vector<tp_elem> elems;
     std::vector<tp_misalign> mis;
+    std::vector<double> aux;  // array fields of the elements
     Schedule sched;
 
     // Element `i` as materialised at turn `turn`.
@@ -848,7 +1015,7 @@ struct Lattice {
             }
         }
         const tp_misalign* m = (e.misalign_index >= 0) ? &mis[size_t(e.misalign_index)] : nullptr;
-        return make_elem<double>(e, m);
+        return make_elem<double>(e, m, aux.empty() ? nullptr : aux.data());
     }
 };
 

@@ -52,7 +52,9 @@ TPO_CNT_TRANSC(tan)
 TPO_CNT_TRANSC(asin)
 TPO_CNT_TRANSC(atan)
 #undef TPO_CNT_TRANSC
-inline Cnt exp(Cnt a) { g_flops += TP_FLOPS_PER_TRANSCENDENTAL; g_transc += 1; return Cnt(std::exp(a.v)); }
+inline Cnt exp(Cnt a) { g_flops += TP_FLOPS_PER_TRANSCENDENTAL; g_transc += 1; return Cnt(tpo::exp(a.v)); }
+inline Cnt sinh(Cnt a) { g_flops += TP_FLOPS_PER_TRANSCENDENTAL; g_transc += 1; return Cnt(tpo::sinh(a.v)); }
+inline Cnt cosh(Cnt a) { g_flops += TP_FLOPS_PER_TRANSCENDENTAL; g_transc += 1; return Cnt(tpo::cosh(a.v)); }
 
 // ---------------------------------------------------------------------------
 // Forward-mode dual number with one tangent (independent AD of the oracle).
@@ -77,7 +79,9 @@ inline D1 cos(D1 a) { return D1(tpo::cos(a.v), -tpo::sin(a.v) * a.d); }
 inline D1 tan(D1 a) { double t = tpo::tan(a.v); return D1(t, (1.0 + t * t) * a.d); }
 inline D1 asin(D1 a) { return D1(tpo::asin(a.v), a.d / std::sqrt(1.0 - a.v * a.v)); }
 inline D1 atan(D1 a) { return D1(tpo::atan(a.v), a.d / (1.0 + a.v * a.v)); }
-inline D1 exp(D1 a) { double e = std::exp(a.v); return D1(e, e * a.d); }
+inline D1 exp(D1 a) { double e = tpo::exp(a.v); return D1(e, e * a.d); }
+inline D1 sinh(D1 a) { return D1(tpo::sinh(a.v), tpo::cosh(a.v) * a.d); }
+inline D1 cosh(D1 a) { return D1(tpo::cosh(a.v), tpo::sinh(a.v) * a.d); }
 }  // namespace tpo
 
 using namespace tpo;
@@ -96,8 +100,13 @@ struct Inputs {
     const double* svalues;
 };
 
+// Array fields of the elements of the next calls (tp_lattice_create_ex's aux),
+// set by orc_set_aux.
+std::vector<double> g_aux;
+
 Lattice build_lattice(const Inputs& in) {
     Lattice lat;
+    lat.aux = g_aux;
     lat.elems.assign(in.elems, in.elems + in.ne);
     if (in.nmis > 0) lat.mis.assign(in.mis, in.mis + in.nmis);
     if (in.nfields > 0) {
@@ -121,7 +130,7 @@ Elem<T> elem_at(const Lattice& lat, int64_t i, int32_t turn) {
                     apply_field(e, lat.sched.fields[2 * j + 1], lat.sched.values[size_t(row * nf + j)]);
     }
     const tp_misalign* m = (e.misalign_index >= 0) ? &lat.mis[size_t(e.misalign_index)] : nullptr;
-    return make_elem<T>(e, m);
+    return make_elem<T>(e, m, lat.aux.empty() ? nullptr : lat.aux.data());
 }
 
 }  // namespace
@@ -131,6 +140,13 @@ extern "C" {
 double orc_beam_beti(double energy, double mass) { return beam_beti(energy, mass); }
 
 int orc_max_threads(void) { return omp_get_max_threads(); }
+
+// The aux array (array fields of StrongGaussianBeam, LongitudinalWake and
+// Wiggler elements) used by the following calls; n = 0 clears it.
+void orc_set_aux(const double* aux, int64_t n) {
+    if (n > 0 && aux) g_aux.assign(aux, aux + n);
+    else g_aux.clear();
+}
 
 // Markstein's reciprocal division q' = RN(q + r*y), q = RN(a*y), r = a - b*q,
 // y = RN(1/b), compared with IEEE a/b on n pairs: returns the number that differ.
@@ -148,7 +164,7 @@ int64_t orc_check_rcp_div(const double* a, const double* b, int64_t n) {
 }
 
 // The shared transcendental functions (which: 0 asin, 1 sin, 2 cos, 3 tan,
-// 4 atan) and the C library's, on n arguments, for the accuracy tests.
+// 4 atan, 5 exp, 6 expm1, 7 sinh, 8 cosh) and the C library's, on n arguments, for the accuracy tests.
 void orc_libm(int32_t which, const double* x, int64_t n, double* ours, double* clib) {
     for (int64_t i = 0; i < n; ++i) {
         switch (which) {
@@ -156,6 +172,10 @@ void orc_libm(int32_t which, const double* x, int64_t n, double* ours, double* c
             case 1: ours[i] = tp::libm::sin(x[i]); clib[i] = std::sin(x[i]); break;
             case 2: ours[i] = tp::libm::cos(x[i]); clib[i] = std::cos(x[i]); break;
             case 3: ours[i] = tp::libm::tan(x[i]); clib[i] = std::tan(x[i]); break;
+            case 5: ours[i] = tp::libm::exp(x[i]); clib[i] = std::exp(x[i]); break;
+            case 6: ours[i] = tp::libm::expm1(x[i]); clib[i] = std::expm1(x[i]); break;
+            case 7: ours[i] = tp::libm::sinh(x[i]); clib[i] = std::sinh(x[i]); break;
+            case 8: ours[i] = tp::libm::cosh(x[i]); clib[i] = std::cosh(x[i]); break;
             default: ours[i] = tp::libm::atan(x[i]); clib[i] = std::atan(x[i]); break;
         }
     }

@@ -275,3 +275,157 @@ def atan(x):
         return x - x * (s1 + s2)
     r = ATANHI[idx] - ((x * (s1 + s2) - ATANLO[idx]) - x)
     return _neg(r) if negx else r
+
+
+# exp, expm1, sinh, cosh (fdlibm method; same reduction, polynomials and
+# branch points as tp_libm.h)
+LN2_HI, LN2_LO, INV_LN2 = 6.93147180369123816490e-01, 1.90821492927058770002e-10, 1.44269504088896338700e+00
+EXP_P = [1.66666666666666019037e-01, -2.77777777770155933842e-03, 6.61375632143793436117e-05,
+         -1.65339022054652515390e-06, 4.13813679705723846039e-08]
+EXP_OVER, EXP_UNDER = 7.09782712893383973096e+02, -7.45133219101941108420e+02
+EM1_Q = [-3.33333333333331316428e-02, 1.58730158725481460165e-03, -7.93650757867487942473e-05,
+         4.00821782732936239552e-06, -2.01099218183624371326e-07]
+TWO_M1000 = 9.33263618503218878990e-302
+
+
+def _add_expo(y, k):
+    return _from((_bits(y) + (k << 52)) & 0xffffffffffffffff)
+
+
+def _trunc(v):
+    return int(v)  # C conversion: toward zero
+
+
+def exp(x):
+    hx = _hix(x)
+    neg = _signbit(x) == 1
+    if hx >= 0x40862E42:
+        if hx >= 0x7ff00000:
+            if _bits(x) & 0x000fffffffffffff:
+                return x + x
+            return 0.0 if neg else x
+        if x > EXP_OVER:
+            return math.inf
+        if x < EXP_UNDER:
+            return 0.0
+    hi = lo = 0.0
+    k = 0
+    if hx > 0x3fd62e42:
+        if hx < 0x3FF0A2B2:
+            hi = x + LN2_HI if neg else x - LN2_HI
+            lo = -LN2_LO if neg else LN2_LO
+            k = -1 if neg else 1
+        else:
+            k = _trunc(INV_LN2 * x + (-0.5 if neg else 0.5))
+            t = float(k)
+            hi = x - t * LN2_HI
+            lo = t * LN2_LO
+        r = hi - lo
+    elif hx < 0x3e300000:
+        return 1.0 + x
+    else:
+        r = x
+    t = r * r
+    c = r - t * (EXP_P[0] + t * (EXP_P[1] + t * (EXP_P[2] + t * (EXP_P[3] + t * EXP_P[4]))))
+    if k == 0:
+        return 1.0 - ((r * c) / (c - 2.0) - r)
+    y = 1.0 - ((lo - (r * c) / (2.0 - c)) - hi)
+    if k >= -1021:
+        return _add_expo(y, k)
+    return _add_expo(y, k + 1000) * TWO_M1000
+
+
+def expm1(x):
+    hx = _hix(x)
+    neg = _signbit(x) == 1
+    if hx >= 0x4043687A:
+        if hx >= 0x40862E42:
+            if hx >= 0x7ff00000:
+                if _bits(x) & 0x000fffffffffffff:
+                    return x + x
+                return -1.0 if neg else x
+            if x > EXP_OVER:
+                return math.inf
+        if neg:
+            return -1.0
+    c = 0.0
+    k = 0
+    if hx > 0x3fd62e42:
+        if hx < 0x3FF0A2B2:
+            if not neg:
+                hi, lo, k = x - LN2_HI, LN2_LO, 1
+            else:
+                hi, lo, k = x + LN2_HI, -LN2_LO, -1
+        else:
+            k = _trunc(INV_LN2 * x + (-0.5 if neg else 0.5))
+            t = float(k)
+            hi = x - t * LN2_HI
+            lo = t * LN2_LO
+        x = hi - lo
+        c = (hi - x) - lo
+    elif hx < 0x3c900000:
+        return x
+    hfx = 0.5 * x
+    hxs = x * hfx
+    r1 = 1.0 + hxs * (EM1_Q[0] + hxs * (EM1_Q[1] + hxs * (EM1_Q[2] + hxs * (EM1_Q[3] + hxs * EM1_Q[4]))))
+    t = 3.0 - r1 * hfx
+    e = hxs * ((r1 - t) / (6.0 - x * t))
+    if k == 0:
+        return x - (x * e - hxs)
+    e = x * (e - c) - c
+    e = e - hxs
+    if k == -1:
+        return 0.5 * (x - e) - 0.5
+    if k == 1:
+        if x < -0.25:
+            return -2.0 * (e - (x + 0.5))
+        return 1.0 + 2.0 * (x - e)
+    if k <= -2 or k > 56:
+        y = 1.0 - (e - x)
+        return _add_expo(y, k) - 1.0
+    if k < 20:
+        t1 = _from((0x3ff00000 - (0x200000 >> k)) << 32)
+        return _add_expo(t1 - (e - x), k)
+    t2 = _from(((0x3ff - k) << 20) << 32)
+    y = x - (e + t2)
+    y = y + 1.0
+    return _add_expo(y, k)
+
+
+def sinh(x):
+    ix = _hix(x)
+    if ix >= 0x7ff00000:
+        return x + x
+    h = -0.5 if _signbit(x) else 0.5
+    ax = abs(x)
+    if ix < 0x40360000:
+        if ix < 0x3e300000:
+            return x
+        t = expm1(ax)
+        if ix < 0x3ff00000:
+            return h * (2.0 * t - (t * t) / (t + 1.0))
+        return h * (t + t / (t + 1.0))
+    if ix < 0x40862E42:
+        return h * exp(ax)
+    w = exp(0.5 * ax)
+    return (h * w) * w
+
+
+def cosh(x):
+    ix = _hix(x)
+    if ix >= 0x7ff00000:
+        return x * x
+    ax = abs(x)
+    if ix < 0x3fd62e43:
+        t = expm1(ax)
+        w = 1.0 + t
+        if ix < 0x3c800000:
+            return w
+        return 1.0 + (t * t) / (w + w)
+    if ix < 0x40360000:
+        t = exp(ax)
+        return 0.5 * t + 0.5 / t
+    if ix < 0x40862E42:
+        return 0.5 * exp(ax)
+    w = exp(0.5 * ax)
+    return (0.5 * w) * w

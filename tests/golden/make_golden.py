@@ -207,6 +207,89 @@ def StrongThinGaussianBeam(amplitude, rmssizex, rmssizey, xoffset=0.0, yoffset=0
 # --------------------------------------------------------------------------
 # Maps (src/tracking.jl), written over 6-tuples
 # --------------------------------------------------------------------------
+def LBend(L, angle, e1=0.0, e2=0.0, K=0.0, by_error=0.0, fint1=0.0, fint2=0.0, full_gap=0.0):  # SCelements.jl:366-377
+    return elem("LBEND", L=L, angle=angle, e1=e1, e2=e2, fint1=fint1, fint2=fint2, gap=full_gap,
+                param=[K, by_error] + [0.0] * 6)
+
+
+def StrongGaussianBeam(charge, total_energy, beamsize, npar, xoff, yoff):  # beambeam.jl:101-114
+    return elem("STRONG_GAUSSIAN_BEAM", param=[charge, total_energy, beamsize[0], beamsize[1]] + [0.0] * 4,
+                aux=list(npar) + list(xoff) + list(yoff))
+
+
+def LongitudinalRLCWake(freq=1.0e9, Rshunt=1.0e6, Q0=1.0, scale=0.0):  # wake.jl:14-18
+    return elem("LONGITUDINAL_RLC_WAKE", param=[freq, Rshunt, Q0, scale] + [0.0] * 4)
+
+
+def LongitudinalWake(times, wakefields, fliphalf=-1.0, scale=0.0):  # wake.jl:52-58
+    return elem("LONGITUDINAL_WAKE", param=[fliphalf, scale] + [0.0] * 6, aux=list(times) + list(wakefields))
+
+
+def lbend_body(r, L, grd, b_angle, by_error):  # tracking.jl:1076-1150
+    if L == 0.0:
+        return r
+    p_norm = 1.0 / (1.0 + r[5])
+    Kx = b_angle / L
+    G1 = (Kx * Kx + grd) * p_norm
+    G2 = -grd * p_norm
+    tol = 1.4901161193847656e-08
+    MHD, M12, M21, MVD, M34, M43 = 1.0, L, 0.0, 1.0, L, 0.0
+    arg1 = sqrtG1 = 0.0
+    if abs(G1) >= tol:
+        if G1 > 0.0:
+            sqrtG1 = math.sqrt(G1)
+            arg1 = L * sqrtG1
+            MHD, M12, M21 = fm.cos(arg1), fm.sin(arg1) / sqrtG1, -fm.sin(arg1) * sqrtG1
+        else:
+            sqrtG1 = math.sqrt(-G1)
+            arg1 = L * sqrtG1
+            MHD, M12, M21 = fm.cosh(arg1), fm.sinh(arg1) / sqrtG1, fm.sinh(arg1) * sqrtG1
+    if abs(G2) >= tol:
+        if G2 > 0.0:
+            sq = math.sqrt(G2)
+            a2 = L * sq
+            MVD, M34, M43 = fm.cos(a2), fm.sin(a2) / sq, -fm.sin(a2) * sq
+        else:
+            sq = math.sqrt(-G2)
+            a2 = L * sq
+            MVD, M34, M43 = fm.cosh(a2), fm.sinh(a2) / sq, fm.sinh(a2) * sq
+    x, xpr, y, ypr = r[0], r[1] * p_norm, r[2], r[3] * p_norm
+    dterm = r[5] * p_norm - by_error
+    x_new = MHD * x + M12 * xpr
+    px_new = (M21 * x + MHD * xpr) / p_norm
+    if abs(G1) < tol:
+        x_new += dterm * L * L * Kx / 2
+        px_new += dterm * L * Kx / p_norm
+    elif G1 > 0.0:
+        x_new += dterm * (1.0 - fm.cos(arg1)) * Kx / G1
+        px_new += dterm * fm.sin(arg1) * Kx / (sqrtG1 * p_norm)
+    else:
+        x_new += dterm * (1.0 - fm.cosh(arg1)) * Kx / G1
+        px_new += dterm * fm.sinh(arg1) * Kx / (sqrtG1 * p_norm)
+    y_new = MVD * y + M34 * ypr
+    py_new = (M43 * y + MVD * ypr) / p_norm
+    z_new = r[4] + xpr * xpr * (L + MHD * M12) / 4
+    if abs(G1) >= tol:
+        z_new += (L - MHD * M12) * (x * x * G1 + dterm * dterm * Kx * Kx / G1 - 2 * x * Kx * dterm) / 4
+        z_new += M12 * M21 * (x * xpr - xpr * dterm * Kx / G1) / 2
+        z_new += Kx * x * M12 + xpr * (1.0 - MHD) * Kx / G1 + dterm * (L - M12) * Kx * Kx / G1
+    z_new += ((L - MVD * M34) * y * y * G2 + ypr * ypr * (L + MVD * M34)) / 4
+    z_new += M34 * M43 * y * ypr / 2
+    return (x_new, px_new, y_new, py_new, z_new, r[5])
+
+
+def interpolate(x, xs, ys):  # _linear_interpolate, wake.jl:68-84
+    if x <= xs[0]:
+        return ys[0] + (ys[1] - ys[0]) / (xs[1] - xs[0]) * (x - xs[0])
+    if x >= xs[-1]:
+        n = len(xs)
+        return ys[n - 1] + (ys[n - 1] - ys[n - 2]) / (xs[n - 1] - xs[n - 2]) * (x - xs[n - 1])
+    for i in range(1, len(xs)):
+        if x < xs[i]:
+            return ys[i - 1] + (ys[i] - ys[i - 1]) / (xs[i] - xs[i - 1]) * (x - xs[i - 1])
+    return ys[-1]
+
+
 def lost_check(r):  # tracking.jl:49-52
     return (math.isnan(r[0]) or abs(r[0]) > COORD_LIMIT or abs(r[2]) > COORD_LIMIT
             or abs(r[1]) > ANGLE_LIMIT or abs(r[3]) > ANGLE_LIMIT)
@@ -525,8 +608,49 @@ def apply_pass(e, r, beti):
         amp, sx, sy, xo, yo = e["param"][:5]
         sx2, sy2 = max(sx * sx, EPS), max(sy * sy, EPS)
         dx, dy = r[0] - xo, r[2] - yo
-        g = amp * math.exp(-0.5 * (dx * dx / sx2 + dy * dy / sy2))
+        g = amp * fm.exp(-0.5 * (dx * dx / sx2 + dy * dy / sy2))
         return (r[0], r[1] - g * dx / sx2, r[2], r[3] - g * dy / sy2, r[4], r[5])
+    if kind == "LBEND":  # tracking.jl:1152-1170
+        if e["L"] == 0.0:
+            return nan6()
+        irho = e["angle"] / e["L"]
+        r = edge(r, irho, e["e1"], e["fint1"], e["gap"], 1, False)
+        r = lbend_body(r, e["L"], e["param"][0], e["angle"], e["param"][1])
+        return edge(r, irho, e["e2"], e["fint2"], e["gap"], 1, True)
+    if kind == "STRONG_GAUSSIAN_BEAM":  # tracking.jl:1621-1641
+        a = e["aux"]
+        nz = len(a) // 3
+        if nz <= 0:
+            return r
+        sx2, sy2 = max(e["param"][2] ** 2, EPS), max(e["param"][3] ** 2, EPS)
+        factor = e["param"][0] / max(abs(e["param"][1]), EPS)
+        px, py = r[1], r[3]
+        for i in range(nz):
+            dx, dy = r[0] - a[nz + i], r[2] - a[2 * nz + i]
+            g = a[i] * fm.exp(-0.5 * (dx * dx / sx2 + dy * dy / sy2))
+            px -= factor * g * dx / sx2
+            py -= factor * g * dy / sy2
+        return (r[0], px, r[2], py, r[4], r[5])
+    if kind == "LONGITUDINAL_RLC_WAKE":  # tracking.jl:1647-1654, wake.jl:27-37
+        freq, rsh, q0, scale = e["param"][:4]
+        if scale == 0.0:
+            return r
+        t = min(r[4] / C_LIGHT, 0.0)
+        q0p = math.sqrt(q0 * q0 - 0.25)
+        w0 = TWO_PI * freq
+        w0p = w0 / q0 * q0p
+        wf = 0.0 if t > 0.0 else rsh * w0 / q0 * (fm.cos(w0p * t) + fm.sin(w0p * t) / (2 * q0p)) * \
+            fm.exp(w0 * t / (2 * q0))
+        return (r[0], r[1], r[2], r[3], r[4], r[5] - scale * wf)
+    if kind == "LONGITUDINAL_WAKE":  # tracking.jl:1656-1663, wake.jl:86-91
+        flip, scale = e["param"][:2]
+        if scale == 0.0:
+            return r
+        n = len(e["aux"]) // 2
+        xs, ys = e["aux"][:n], e["aux"][n:]
+        t = r[4] / C_LIGHT
+        wf = 0.0 if t > xs[0] * flip else interpolate(t * flip, xs, ys)
+        return (r[0], r[1], r[2], r[3], r[4], r[5] - scale * wf)
     raise ValueError(kind)
 
 
@@ -620,6 +744,17 @@ def extra_cases(energy):
         ("ExactSBendKick", [eb_kick]),
         ("ExactSBendNoSteps", [eb0]),
         ("RFNoEnergy", [RFCavity(0.2, 1.0e6, 500.0e6)]),
+        ("LBendFocusing", [LBend(0.9, 0.15, 0.03, 0.02, K=0.8, by_error=1e-4, fint1=0.5, fint2=0.4,
+                                 full_gap=0.05)]),
+        ("LBendDefocusing", [LBend(0.9, 0.15, 0.03, 0.02, K=-0.9)]),
+        ("LBendNoGradient", [LBend(1.2, 1e-5, 0.0, 0.0)]),
+        ("StrongGaussianBeam", [StrongGaussianBeam(1.0e-3, 6.0e9, (3e-4, 4e-4), [0.2, 0.5, 0.3],
+                                                   [1e-5, 0.0, -2e-5], [0.0, 3e-5, -1e-5])]),
+        ("LongitudinalRLCWake", [LongitudinalRLCWake(1.2e9, 2.0e5, 3.5, 2e-19)]),
+        ("LongitudinalWake", [LongitudinalWake([0.0, 2e-12, 5e-12, 1e-11, 3e-11],
+                                               [1e13, 6e12, 2e12, -1e12, 0.0], fliphalf=-3.0, scale=1e-19)]),
+        ("LongitudinalWakeUnsorted", [LongitudinalWake([0.0, 5e-12, 2e-12, 1e-11], [1e13, 2e12, 6e12, -1e12],
+                                                       fliphalf=-4.0, scale=2e-19)]),
     ]
 
 

@@ -35,6 +35,7 @@ def lib():
         _lib.orc_pass_elements.argtypes = [P, C.c_int64, P, C.c_int64, P, C.c_int64, C.c_double, C.c_int32]
         _lib.orc_submap.argtypes = [C.c_int32, P, C.c_double, C.c_double, C.c_double]
         _lib.orc_max_threads.restype = C.c_int
+        _lib.orc_set_aux.argtypes = [P, C.c_int64]
     return _lib
 
 
@@ -43,14 +44,19 @@ def _ptr(a):
 
 
 def _packed(lat):
-    """(elems, n, mis, nmis, keep) from a Lattice, a list of dicts or a TpElem array."""
+    """(elems, n, mis, nmis) from a Lattice or a list of element dicts; the
+    elements' array fields are handed to the oracle (orc_set_aux) for the call
+    that follows."""
     if hasattr(lat, "pack"):
-        arr, n, marr, nm = lat.pack()
-        return arr, n, (marr if nm else None), nm
-    import importlib
-    abi = importlib.import_module("trackpad_b200._abi")
-    arr = abi.elem_array(lat)
-    return arr, len(lat), None, 0
+        arr, n, marr, nm, aux = lat.pack()
+    else:
+        import importlib
+        abi = importlib.import_module("trackpad_b200._abi")
+        arr, aux = abi.elem_array_aux(lat)
+        n, marr, nm = len(lat), None, 0
+    aux = np.ascontiguousarray(aux, dtype=np.float64)
+    lib().orc_set_aux(aux.ctypes.data_as(P) if len(aux) else None, len(aux))  # the oracle copies it
+    return arr, n, (marr if nm else None), nm
 
 
 def _schedule(sched):

@@ -103,9 +103,12 @@ def test_flop_model_matches_oracle_op_count(lat_name, golden):
         lats = [(tp.Lattice([]), 3.5e9)]
         lats = []
         for c in golden["cases"]:
-            arr = abi.elem_array(c["elements"])
+            arr, aux = abi.elem_array_aux(c["elements"])
+            aux = np.asarray(aux, dtype=np.float64)
             h = C.c_void_p()
-            assert abi.lib().tp_lattice_create(arr, len(c["elements"]), None, 0, C.byref(h)) == 0
+            assert abi.lib().tp_lattice_create_ex(arr, len(c["elements"]), None, 0,
+                                                  aux.ctypes.data_as(C.c_void_p) if len(aux) else None, len(aux),
+                                                  C.byref(h)) == 0
             out = np.zeros(len(c["elements"]))
             abi.lib().tp_lattice_flops(h, out.ctypes.data_as(C.c_void_p))
             ref, _ = oracle_ref.count_flops(c["elements"], float.fromhex(c["beti"]))

@@ -1,9 +1,8 @@
 """GPU tracking against the oracle and the golden fixtures, through the C ABI.
 
 Default build (no FMA contraction; transcendental functions from the shared
-fdlibm-method implementation): coordinates, loss flags, turn and element of
-loss are bit-identical to the oracle for every map except those that call exp
-(StrongThinGaussianBeam), and there within 1e-12 relative.
+fdlibm-method implementation, exp/sinh/cosh included): coordinates, loss
+flags, turn and element of loss are bit-identical to the oracle for every map.
 
 FMA-contraction build (opt-in): 1e-9 relative (per coordinate, scaled by the
 column's largest magnitude) after one turn on regular orbits -- the exact
@@ -19,7 +18,7 @@ from conftest import col_rel_err, tp, unhex
 pytestmark = pytest.mark.gpu
 W = __import__("trackpad_b200.workloads", fromlist=["x"])
 
-USES_EXP = {"StrongThinGaussianBeam"}
+USES_EXP = set()  # exp now comes from the shared libm too: no exception left
 
 
 def _run_case(c, contract):
@@ -334,6 +333,27 @@ def test_batched_time_dependent_equals_lattice_by_lattice():
             rl = np.zeros(counts[i], np.int64)
             tp.ringpass_(rc, lat, beam, rl, 6, turn=turn0, aperture=0.02, schedule=1)
             assert np.array_equal(c[s], rc) and np.array_equal(l[s], rl)
+
+
+def test_array_field_kinds_bitwise():
+    """LBend (both signs of the gradient), StrongGaussianBeam slices, the
+    resonator wake and sorted / unsorted tabulated wakes, over a beam whose z
+    spans the wake tables, against the oracle bit for bit."""
+    lat = tp.Lattice([
+        tp.LBend(0.9, 0.15, 0.03, 0.02, K=0.8, by_error=1e-4, fint1=0.5, fint2=0.4, full_gap=0.05),
+        tp.Drift(0.5),
+        tp.LBend(0.9, 0.15, 0.03, 0.02, K=-0.9),
+        tp.StrongGaussianBeam(1e-3, 0.511e6, 1, 10, 6e9, (3e-4, 4e-4), nzslice=4,
+                              zslice_npar=[0.1, 0.4, 0.3, 0.2], xoffsets=[1e-5, 0, -2e-5, 3e-5]),
+        tp.LongitudinalRLCWake(freq=1.2e9, Rshunt=2e5, Q0=3.5, scale=2e-19),
+        tp.LongitudinalWake(list(np.linspace(0, 3e-11, 40)), list(1e13 * np.cos(np.linspace(0, 6, 40))),
+                            fliphalf=-1.0, scale=1e-19),
+        tp.LongitudinalWake([0.0, 5e-12, 2e-12, 1e-11], [1e13, 2e12, 6e12, -1e12], fliphalf=-1.0, scale=2e-19),
+        tp.Quadrupole(0.4, 1.1),
+    ])
+    beam = tp.Beam(3.5e9)
+    c = W.gaussian(4096, seed=77, sigma=(1e-4, 1e-5, 1e-4, 1e-5, 3e-3, 1e-4))
+    _compare(lat, beam, c, 3, 0.05, 1e-12)
 
 
 def test_unsupported_schedule_outside_range():

@@ -49,7 +49,7 @@ def test_pack_roundtrip():
 def test_misalignment_packs_into_side_table():
     d = tp.Drift(1.0, t1=[1e-3, 0, 0, 0, 0, 0])
     lat = tp.Lattice([tp.Drift(1.0), d])
-    arr, n, marr, nm = lat.pack()
+    arr, n, marr, nm, aux = lat.pack()
     assert nm == 1 and arr[1].misalign_index == 0 and marr[0].t1[0] == 1e-3
 
 

@@ -8,7 +8,7 @@ import pytest
 
 import oracle_ref
 
-FUNCS = {"asin": 0, "sin": 1, "cos": 2, "tan": 3, "atan": 4}
+FUNCS = {"asin": 0, "sin": 1, "cos": 2, "tan": 3, "atan": 4, "exp": 5, "expm1": 6, "sinh": 7, "cosh": 8}
 
 
 def ulp_diff(a, b):
@@ -43,6 +43,10 @@ def samples(lo, hi, n, rng, log=False):
     ("cos", [(-np.pi / 4, np.pi / 4, False), (1e-12, 1.0, True), (-50.0, 50.0, False), (1.0, 1e5, True)]),
     ("tan", [(-np.pi / 4, np.pi / 4, False), (1e-12, 1.0, True), (-1.5, 1.5, False), (1.0, 1e5, True)]),
     ("atan", [(-3.0, 3.0, False), (1e-12, 1e12, True), (0.4, 2.5, False)]),
+    ("exp", [(-1.0, 1.0, False), (1e-12, 1.0, True), (-700.0, 700.0, False), (-30.0, 30.0, False)]),
+    ("expm1", [(-1.0, 1.0, False), (1e-12, 1.0, True), (-40.0, 700.0, False), (-0.5, 0.5, False)]),
+    ("sinh", [(-1.0, 1.0, False), (1e-12, 1.0, True), (-25.0, 25.0, False), (20.0, 700.0, False)]),
+    ("cosh", [(-1.0, 1.0, False), (1e-12, 0.4, True), (-25.0, 25.0, False), (20.0, 700.0, False)]),
 ])
 def test_within_one_ulp_of_c_library(name, ranges):
     rng = np.random.Generator(np.random.Philox(7))
@@ -50,7 +54,11 @@ def test_within_one_ulp_of_c_library(name, ranges):
         x = samples(lo, hi, 200000, rng, log)
         ours, clib = run(name, x)
         d = ulp_diff(ours, clib)
-        assert d.max() <= 1, f"{name} on [{lo}, {hi}]: {d.max()} ulp"
+        # sinh and cosh are the fdlibm method over this exp/expm1 (within 1 ulp
+        # of the C library's), so a rare result sits 2 ulp away
+        bound = 2 if name in ("sinh", "cosh") else 1
+        assert d.max() <= bound, f"{name} on [{lo}, {hi}]: {d.max()} ulp"
+        assert (d <= 1).mean() > 0.999, f"{name}: too many results beyond 1 ulp"
         assert (d == 0).mean() > 0.8, f"{name}: too many 1-ulp differences"
 
 
@@ -60,6 +68,8 @@ def test_special_values():
         same = (ours == clib) | (np.isnan(ours) & np.isnan(clib))
         if name == "asin":
             same[3:5] = np.isnan(ours[3:5])
+        if name in ("exp", "expm1", "sinh", "cosh"):  # finite non-zero arguments: within 1 ulp
+            same[5:] |= ulp_diff(ours[5:], clib[5:]) <= 1
         assert same.all(), (name, ours, clib)
 
 

@@ -9,7 +9,8 @@ from .elements import (AbstractElement, AccelCavity, Corrector, CrabCavity, Drif
                        HKicker, InvLorentzBoost, LongitudinalRFMap, LorentzBoost, M_ELECTRON, M_PROTON, Marker,
                        Octupole, OctupoleSC, Quadrupole, QuadrupoleSC, RBend, RBendSC, RFCavity, SBend, SBendSC,
                        Sextupole, SextupoleSC, Solenoid, SpaceCharge, StrongThinGaussianBeam, ThinMultipole,
-                       Translation, VKicker, YRotation)
+                       Translation, VKicker, YRotation, LBend, StrongGaussianBeam, LongitudinalRLCWake,
+                       LongitudinalWake)
 from .tracking import (Batch, Beam, Lattice, Time, TimeContext, TimeDependentParam, TimeVaryingElement, Turn,
                        adjoint_stats, beti, context, last_stats, linepass_, materialize, one_turn_jacobian,
                        probe_fp64_peak, ringpass_, ringpass_adjoint, spos, timed)

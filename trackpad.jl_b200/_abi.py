@@ -25,7 +25,8 @@ KINDS = [
     "MARKER", "DRIFT", "QUADRUPOLE", "SEXTUPOLE", "OCTUPOLE", "THIN_MULTIPOLE", "SBEND", "EXACT_SBEND",
     "RFCAVITY", "SOLENOID", "CORRECTOR", "TRANSLATION", "YROTATION", "CRAB_CAVITY", "ACCEL_CAVITY",
     "LONGITUDINAL_RF_MAP", "LORENTZ_BOOST", "INV_LORENTZ_BOOST", "SPACE_CHARGE", "DRIFT_SC", "QUADRUPOLE_SC",
-    "SEXTUPOLE_SC", "OCTUPOLE_SC", "SBEND_SC", "STRONG_THIN_GAUSSIAN_BEAM",
+    "SEXTUPOLE_SC", "OCTUPOLE_SC", "SBEND_SC", "STRONG_THIN_GAUSSIAN_BEAM", "LBEND", "WIGGLER",
+    "STRONG_GAUSSIAN_BEAM", "LONGITUDINAL_RLC_WAKE", "LONGITUDINAL_WAKE",
 ]
 KIND = {name: i for i, name in enumerate(KINDS)}
 
@@ -87,13 +88,22 @@ class TpAdjointStats(C.Structure):
     ]
 
 
-def elem_from_dict(d):
-    """Fill a TpElem from a dict with reference field names (kind given by name)."""
+def elem_from_dict(d, aux=None):
+    """Fill a TpElem from a dict with reference field names (kind given by name).
+    An "aux" entry (list of floats: the element's array fields) is appended to
+    `aux` and referenced by iparam[0] (offset) and iparam[1] (length)."""
     e = TpElem()
     e.kind = KIND[d["kind"]] if isinstance(d["kind"], str) else int(d["kind"])
     e.misalign_index = -1
     for key, val in d.items():
         if key == "kind":
+            continue
+        if key == "aux":
+            if aux is None:
+                raise ValueError("this element has array fields: pack it with elem_array_aux")
+            e.iparam[0] = len(aux)
+            e.iparam[1] = len(val)
+            aux.extend(float(v) for v in val)
             continue
         if key in ("polynom_a", "polynom_b", "kick_angle", "param", "iparam"):
             arr = getattr(e, key)
@@ -105,10 +115,16 @@ def elem_from_dict(d):
 
 
 def elem_array(dicts):
+    return elem_array_aux(dicts)[0]
+
+
+def elem_array_aux(dicts):
+    """(TpElem array, aux list) of a list of element dicts."""
     arr = (TpElem * max(len(dicts), 1))()
+    aux = []
     for i, d in enumerate(dicts):
-        arr[i] = d if isinstance(d, TpElem) else elem_from_dict(d)
-    return arr
+        arr[i] = d if isinstance(d, TpElem) else elem_from_dict(d, aux)
+    return arr, aux
 
 
 P = C.c_void_p
@@ -122,6 +138,7 @@ _SIGS = {
     "tp_last_stats": (C.c_int, [P, C.POINTER(TpStats)]),
     "tp_beam_beti": (C.c_int, [C.c_double, C.c_double, C.POINTER(C.c_double)]),
     "tp_lattice_create": (C.c_int, [P, C.c_int64, P, C.c_int64, C.POINTER(P)]),
+    "tp_lattice_create_ex": (C.c_int, [P, C.c_int64, P, C.c_int64, P, C.c_int64, C.POINTER(P)]),
     "tp_lattice_destroy": (C.c_int, [P]),
     "tp_lattice_length": (C.c_int, [P, C.POINTER(C.c_int64)]),
     "tp_lattice_flops": (C.c_int, [P, P]),

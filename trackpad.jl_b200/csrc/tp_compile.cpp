@@ -31,11 +31,17 @@ bool has_misalign_fields(int kind) {
     switch (kind) {
         case TP_DRIFT: case TP_DRIFT_SC: case TP_QUADRUPOLE: case TP_SEXTUPOLE: case TP_OCTUPOLE:
         case TP_THIN_MULTIPOLE: case TP_SBEND: case TP_EXACT_SBEND: case TP_SOLENOID: case TP_CORRECTOR:
-        case TP_QUADRUPOLE_SC: case TP_SEXTUPOLE_SC: case TP_OCTUPOLE_SC: case TP_SBEND_SC:
+        case TP_QUADRUPOLE_SC: case TP_SEXTUPOLE_SC: case TP_OCTUPOLE_SC: case TP_SBEND_SC: case TP_LBEND:
+        case TP_WIGGLER:
             return true;
         default:
             return false;
     }
+}
+
+// Kinds whose arrays live in aux[iparam[0] .. iparam[0] + iparam[1]).
+bool uses_aux(int kind) {
+    return kind == TP_STRONG_GAUSSIAN_BEAM || kind == TP_LONGITUDINAL_WAKE || kind == TP_WIGGLER;
 }
 
 bool uses_order(int kind) {
@@ -51,8 +57,26 @@ bool uses_order(int kind) {
 struct Rec {
     RecHdr h{};
     double w[MAX_REC_WORDS]{};
-    int nw = 0;  // payload words
+    int nw = 0;                // fixed payload words
+    std::vector<double> tail;  // arrays after the fixed words
 };
+
+// edge_fringe_entrance / _exit constants (tracking.jl:162-172, 196-206):
+// fx = irho tan(e), the edge angle and the fringe correction irho gap fint
+// (1 + sin^2 e) / cos e (zero without fint, gap or method).
+void edge_consts(double irho, double gap, int method, double ang, double fint, double* fx, double* eang,
+                 double* fc) {
+    double corr;
+    if (fint == 0.0 || gap == 0.0 || method == 0) {
+        corr = 0.0;
+    } else {
+        double sedge = libm::sin(ang), cedge = libm::cos(ang);
+        corr = irho * gap * fint * (1.0 + sedge * sedge) / cedge;
+    }
+    *fx = irho * libm::tan(ang);
+    *eang = ang;
+    *fc = corr;
+}
 
 // symplectic4_pass / symplectic4_bend_pass slice constants (src/tracking.jl:325-329).
 void yoshida_consts(double L, int n, double* L1, double* L2, double* K1, double* K2) {
@@ -73,7 +97,7 @@ void fold_kick(const tp_elem& e, double* pa, double* pb) {
 
 }  // namespace
 
-int validate_elem(const tp_elem& e, int64_t idx, int64_t nmis, std::string* err) {
+int validate_elem(const tp_elem& e, int64_t idx, int64_t nmis, std::string* err, const AuxView& aux) {
     auto fail = [&](const char* what) {
         *err = "element " + std::to_string(idx) + ": " + what;
         return TP_EINVAL;
@@ -81,6 +105,30 @@ int validate_elem(const tp_elem& e, int64_t idx, int64_t nmis, std::string* err)
     if (e.kind < 0 || e.kind >= TP_KIND_COUNT) {
         *err = "element " + std::to_string(idx) + ": unknown kind " + std::to_string(e.kind);
         return TP_EUNSUPPORTED;
+    }
+    if (uses_aux(e.kind)) {
+        const int64_t off = e.iparam[0], len = e.iparam[1];
+        if (off < 0 || len < 0 || off + len > aux.n || (len > 0 && aux.p == nullptr))
+            return fail("array fields outside the aux array (tp_lattice_create_ex)");
+        if (len > 60000) {
+            *err = "element " + std::to_string(idx) + ": array fields longer than 60000 words";
+            return TP_ERANGE;
+        }
+        if (e.kind == TP_STRONG_GAUSSIAN_BEAM && len % 3 != 0)
+            return fail("StrongGaussianBeam arrays: zslice_npar, xoffsets, yoffsets of nzslice each");
+        if (e.kind == TP_LONGITUDINAL_WAKE && (len % 2 != 0 || len < 4))
+            return fail("LongitudinalWake needs times and wakefields of the same length >= 2");
+        if (e.kind == TP_WIGGLER) {
+            if (len < 3) return fail("Wiggler arrays: NHharm, NVharm, rad, By, Bx");
+            const double* a = aux.p + off;
+            const int64_t nh = int64_t(a[0]), nv = int64_t(a[1]);
+            if (nh < 0 || nv < 0 || a[0] != double(nh) || a[1] != double(nv) || 3 + 6 * (nh + nv) != len)
+                return fail("Wiggler arrays: length must be 3 + 6 NHharm + 6 NVharm");
+            if (!(e.param[0] > 0.0)) return fail("Wiggler lw must be positive");
+        }
+    }
+    if (e.kind == TP_LBEND && e.L == 0.0) {
+        // pass!(::LBend) returns NaN for L == 0 (tracking.jl:1158-1160); accepted, compiled to a NaN map
     }
     if (uses_order(e.kind) && (e.max_order < 0 || e.max_order > 3))
         return fail("max_order must be in 0..3 (polynom_a/polynom_b hold 4 coefficients)");
@@ -94,7 +142,7 @@ int validate_elem(const tp_elem& e, int64_t idx, int64_t nmis, std::string* err)
 }
 
 // Compile one element.  Returns the record words (header + payload).
-static Rec compile_rec(const tp_elem& e) {
+static Rec compile_rec(const tp_elem& e, const AuxView& aux) {
     Rec r;
     r.h.kind = DK_IDENTITY;
     r.h.order = 0;
@@ -162,18 +210,8 @@ static Rec compile_rec(const tp_elem& e) {
             yoshida_consts(e.L, e.num_int_steps, &r.w[mp::L1], &r.w[mp::L2], &r.w[mp::K1], &r.w[mp::K2]);
             for (int i = 0; i < 4; ++i) { r.w[mp::PA + i] = pa[i]; r.w[mp::PB + i] = pb[i]; }
             r.w[sb::IRHO] = irho;
-            // edge_fringe_entrance / _exit constants (tracking.jl:162-172, 196-206)
             auto edge = [&](int method, double ang, double fint, double* fx, double* eang, double* fc) {
-                double corr;
-                if (fint == 0.0 || e.gap == 0.0 || method == 0) {
-                    corr = 0.0;
-                } else {
-                    double sedge = libm::sin(ang), cedge = libm::cos(ang);
-                    corr = irho * e.gap * fint * (1.0 + sedge * sedge) / cedge;
-                }
-                *fx = irho * libm::tan(ang);
-                *eang = ang;
-                *fc = corr;
+                edge_consts(irho, e.gap, method, ang, fint, fx, eang, fc);
             };
             if (e.fringe_bend_entrance != 0) {
                 r.h.flags |= RF_FRINGE_IN;
@@ -342,10 +380,70 @@ static Rec compile_rec(const tp_elem& e) {
             r.nw = stg::WORDS;
             break;
         }
+        case TP_LBEND: {  // tracking.jl:1152-1170 (edges: method 1), body :1076-1150
+            if (e.L == 0.0) { r.h.kind = DK_NAN; break; }
+            r.h.kind = DK_LBEND;
+            const double kx = e.angle / e.L;  // Kx = b_angle / L, and irho of the edges
+            r.w[lb::L] = e.L;
+            r.w[lb::KX] = kx;
+            r.w[lb::G1C] = kx * kx + e.param[0];
+            r.w[lb::NGRD] = -e.param[0];
+            r.w[lb::BYERR] = e.param[1];
+            r.w[lb::IRHO] = kx;
+            edge_consts(kx, e.gap, 1, e.e1, e.fint1, &r.w[lb::FX_IN], &r.w[lb::E_IN], &r.w[lb::FC_IN]);
+            edge_consts(kx, e.gap, 1, e.e2, e.fint2, &r.w[lb::FX_OUT], &r.w[lb::E_OUT], &r.w[lb::FC_OUT]);
+            if (r.w[lb::FC_IN] == 0.0) r.h.flags |= RF_FC_IN_ZERO;
+            if (r.w[lb::FC_OUT] == 0.0) r.h.flags |= RF_FC_OUT_ZERO;
+            r.nw = lb::WORDS;
+            break;
+        }
+        case TP_STRONG_GAUSSIAN_BEAM: {  // tracking.jl:1621-1641
+            const int64_t nz = e.iparam[1] / 3;
+            if (nz <= 0) { r.h.kind = DK_IDENTITY; break; }
+            r.h.kind = DK_SGB;
+            r.w[sgb::FACTOR] = e.param[0] / jmax_eps(std::fabs(e.param[1]));
+            r.w[sgb::SX2] = jmax_eps(e.param[2] * e.param[2]);
+            r.w[sgb::SY2] = jmax_eps(e.param[3] * e.param[3]);
+            r.w[sgb::NZ] = double(nz);
+            r.nw = sgb::WORDS;
+            r.tail.assign(aux.p + e.iparam[0], aux.p + e.iparam[0] + 3 * nz);
+            break;
+        }
+        case TP_LONGITUDINAL_RLC_WAKE: {  // tracking.jl:1647-1654, elements/wake.jl:27-37
+            if (e.param[3] == 0.0) { r.h.kind = DK_IDENTITY; break; }
+            r.h.kind = DK_RLC_WAKE;
+            const double freq = e.param[0], rsh = e.param[1], q0 = e.param[2];
+            const double q0p = std::sqrt(q0 * q0 - 0.25);
+            const double w0 = TWO_PI * freq;
+            r.w[rlc::SCALE] = e.param[3];
+            r.w[rlc::A] = rsh * w0 / q0;
+            r.w[rlc::W0P] = w0 / q0 * q0p;
+            r.w[rlc::D2Q0P] = 2.0 * q0p;
+            r.w[rlc::W0] = w0;
+            r.w[rlc::D2Q0] = 2.0 * q0;
+            r.nw = rlc::WORDS;
+            break;
+        }
+        case TP_LONGITUDINAL_WAKE: {  // tracking.jl:1656-1663, elements/wake.jl:68-91
+            if (e.param[1] == 0.0) { r.h.kind = DK_IDENTITY; break; }
+            const int64_t n = e.iparam[1] / 2;
+            const double* t = aux.p + e.iparam[0];
+            r.h.kind = DK_TAB_WAKE;
+            bool sorted = true;
+            for (int64_t i = 1; i < n; ++i) sorted = sorted && t[i - 1] <= t[i];
+            r.h.order = sorted ? 1 : 0;  // sorted times: the device finds the segment by bisection
+            r.w[tw::SCALE] = e.param[1];
+            r.w[tw::FLIP] = e.param[0];
+            r.w[tw::T1F] = t[0] * e.param[0];
+            r.w[tw::N] = double(n);
+            r.nw = tw::WORDS;
+            r.tail.assign(t, t + 2 * n);
+            break;
+        }
         default:
             break;
     }
-    r.h.words = uint16_t(HDR_WORDS + r.nw);
+    r.h.words = uint16_t(HDR_WORDS + r.nw + int(r.tail.size()));
     return r;
 }
 
@@ -354,15 +452,18 @@ static void append_rec(const Rec& r, std::vector<double>* out) {
     out->resize(at + r.h.words);
     std::memcpy(out->data() + at, &r.h, sizeof(RecHdr));
     for (int i = 0; i < r.nw; ++i) (*out)[at + HDR_WORDS + i] = r.w[i];
+    for (size_t i = 0; i < r.tail.size(); ++i) (*out)[at + HDR_WORDS + r.nw + i] = r.tail[i];
 }
 
-void compile_record(const tp_elem& e, std::vector<double>* out) { append_rec(compile_rec(e), out); }
+void compile_record(const tp_elem& e, std::vector<double>* out, const AuxView& aux) {
+    append_rec(compile_rec(e, aux), out);
+}
 
-int record_words(const tp_elem& e) { return compile_rec(e).h.words; }
+int record_words(const tp_elem& e, const AuxView& aux) { return compile_rec(e, aux).h.words; }
 
-void scheduled_stub(const tp_elem& e, int32_t slot, std::vector<double>* out) {
+void scheduled_stub(const tp_elem& e, int32_t slot, std::vector<double>* out, const AuxView& aux) {
     Rec r;
-    r.h.kind = compile_rec(e).h.kind;
+    r.h.kind = compile_rec(e, aux).h.kind;
     r.h.flags = RF_SCHEDULED;
     r.h.words = HDR_WORDS;
     r.h.aux = slot;
@@ -397,7 +498,7 @@ void apply_field(tp_elem* e, int field, double v) {
 // transcendental call = TP_FLOPS_PER_TRANSCENDENTAL (20).  Every constant
 // below is checked against the oracle's op-counting scalar in the CPU tests.
 // ---------------------------------------------------------------------------
-double elem_flops(const tp_elem& e, const tp_misalign* mis, bool exact) {
+double elem_flops(const tp_elem& e, const tp_misalign* mis, bool exact, const AuxView& aux) {
     const double TR = TP_FLOPS_PER_TRANSCENDENTAL;
     const double D = exact ? 20.0 : 14.0;           // drift6
     auto kick = [](int m) { return 8.0 * m + 4.0; };  // strthinkick
@@ -472,6 +573,27 @@ double elem_flops(const tp_elem& e, const tp_misalign* mis, bool exact) {
         case TP_LORENTZ_BOOST: return 8.0;
         case TP_INV_LORENTZ_BOOST: return 7.0;
         case TP_STRONG_THIN_GAUSSIAN_BEAM: return 17.0 + TR;
+        case TP_LBEND: {
+            if (e.L == 0.0) return mis_f;
+            // edges (method 1) as for the SBend; body: 57 operations, plus the
+            // focusing terms of each plane whose |G| = |(Kx^2 + K, -K) p_norm| >= sqrt(eps)
+            auto edge = [&](double fint) { return 49.0 + ((fint == 0.0 || e.gap == 0.0) ? 0.0 : 46.0); };
+            const double kx = e.angle / e.L;
+            const double g1 = kx * kx + e.param[0], g2 = -e.param[0];
+            const double tol = 1.4901161193847656e-08;
+            double body = 57.0;
+            if (std::fabs(g1) >= tol) body += 44.0 + 5.0 * TR;
+            if (std::fabs(g2) >= tol) body += 4.0 + 3.0 * TR;
+            return mis_f + 1.0 + edge(e.fint1) + body + edge(e.fint2);
+        }
+        case TP_STRONG_GAUSSIAN_BEAM: {
+            const double nz = double(e.iparam[1] / 3);
+            return nz <= 0.0 ? 0.0 : 3.0 + nz * (17.0 + TR);
+        }
+        case TP_LONGITUDINAL_RLC_WAKE: return e.param[3] == 0.0 ? 0.0 : 21.0 + 3.0 * TR;
+        case TP_LONGITUDINAL_WAKE:
+            // a particle ahead of the wake (z > 0 with fliphalf < 0); one behind adds the interpolation
+            return e.param[1] == 0.0 ? 0.0 : 3.0;
         default: return 0.0;
     }
 }

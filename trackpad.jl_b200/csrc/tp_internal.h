@@ -10,13 +10,19 @@
 
 namespace tp {
 
+// Array fields of the elements (the `aux` argument of tp_lattice_create_ex).
+struct AuxView {
+    const double* p = nullptr;
+    int64_t n = 0;
+};
+
 // Host compiler (tp_compile.cpp)
-int validate_elem(const tp_elem& e, int64_t idx, int64_t nmis, std::string* err);
-void compile_record(const tp_elem& e, std::vector<double>* out);
-int record_words(const tp_elem& e);
-void scheduled_stub(const tp_elem& e, int32_t slot, std::vector<double>* out);
+int validate_elem(const tp_elem& e, int64_t idx, int64_t nmis, std::string* err, const AuxView& aux = AuxView{});
+void compile_record(const tp_elem& e, std::vector<double>* out, const AuxView& aux = AuxView{});
+int record_words(const tp_elem& e, const AuxView& aux = AuxView{});
+void scheduled_stub(const tp_elem& e, int32_t slot, std::vector<double>* out, const AuxView& aux = AuxView{});
 void apply_field(tp_elem* e, int field, double v);
-double elem_flops(const tp_elem& e, const tp_misalign* mis, bool exact);
+double elem_flops(const tp_elem& e, const tp_misalign* mis, bool exact, const AuxView& aux = AuxView{});
 
 // Arguments of one tracking launch.  All pointers are device pointers.
 struct TrackArgs {

@@ -8,7 +8,7 @@
 // written with explicitly rounded IEEE operations only (no fused multiply-add,
 // no contraction), so both produce the same bits.
 //
-// Method: the published fdlibm algorithms (Sun Microsystems, as distributed in
+// Method (exp, expm1, sinh and cosh too, at the end of this file): the published fdlibm algorithms (Sun Microsystems, as distributed in
 // FreeBSD msun and used by Julia's Base.Math for Float64): rational minimax
 // approximation for asin on |x| < 0.5 and the half-angle identity above it;
 // minimax polynomial kernels for sin, cos and tan on [-pi/4, pi/4] with a
@@ -372,6 +372,161 @@ TPM_FN double atan(double x) {
     if (id < 0) return sub(x, mul(x, add(s1, s2)));
     double r = sub(atanhi(id), sub(sub(mul(x, add(s1, s2)), atanlo(id)), x));
     return negx ? neg(r) : r;
+}
+
+// ---------------------------------------------------------------------------
+// exp, expm1, sinh, cosh (fdlibm methods).  exp: x = k ln2 + r with ln2 split
+// in a head and a tail, |r| <= ln2/2, and a minimax polynomial for the
+// rational form r*(exp(r)+1)/(exp(r)-1); expm1: the same reduction with a
+// correction term c for the rounding of r, and a minimax polynomial for the
+// rational form of expm1 on the primary range; sinh and cosh from expm1 for
+// small arguments and from exp otherwise.
+// ---------------------------------------------------------------------------
+constexpr double LN2_HI = 6.93147180369123816490e-01, LN2_LO = 1.90821492927058770002e-10;
+constexpr double INV_LN2 = 1.44269504088896338700e+00;
+constexpr double EXP_P1 = 1.66666666666666019037e-01, EXP_P2 = -2.77777777770155933842e-03,
+                 EXP_P3 = 6.61375632143793436117e-05, EXP_P4 = -1.65339022054652515390e-06,
+                 EXP_P5 = 4.13813679705723846039e-08;
+constexpr double EXP_OVER = 7.09782712893383973096e+02, EXP_UNDER = -7.45133219101941108420e+02;
+constexpr double EM1_Q1 = -3.33333333333331316428e-02, EM1_Q2 = 1.58730158725481460165e-03,
+                 EM1_Q3 = -7.93650757867487942473e-05, EM1_Q4 = 4.00821782732936239552e-06,
+                 EM1_Q5 = -2.01099218183624371326e-07;
+constexpr double TWO_M1000 = 9.33263618503218878990e-302;  // 2^-1000
+
+// y * 2^k by adding k to the biased exponent (y normal, result normal).
+TPM_FN double add_expo(double y, int k) { return from_bits(bits(y) + (uint64_t(int64_t(k)) << 52)); }
+
+TPM_FN double exp(double x) {
+    const uint32_t hx = hix(x);
+    const bool neg_x = (bits(x) >> 63) != 0;
+    if (hx >= 0x40862E42u) {                       // |x| >= 709.78 or not finite
+        if (hx >= 0x7ff00000u) {
+            if (((bits(x) & 0x000fffffffffffffull) != 0)) return add(x, x);  // NaN
+            return neg_x ? 0.0 : x;                 // exp(+-inf)
+        }
+        if (x > EXP_OVER) return from_bits(0x7ff0000000000000ull);  // overflow
+        if (x < EXP_UNDER) return 0.0;
+    }
+    double hi = 0.0, lo = 0.0, r;
+    int k = 0;
+    if (hx > 0x3fd62e42u) {                        // |x| > ln2/2
+        if (hx < 0x3FF0A2B2u) {                    // |x| < 1.5 ln2: k = +-1
+            hi = neg_x ? add(x, LN2_HI) : sub(x, LN2_HI);
+            lo = neg_x ? -LN2_LO : LN2_LO;
+            k = neg_x ? -1 : 1;
+        } else {
+            k = int(add(mul(INV_LN2, x), neg_x ? -0.5 : 0.5));
+            const double t = double(k);
+            hi = sub(x, mul(t, LN2_HI));
+            lo = mul(t, LN2_LO);
+        }
+        r = sub(hi, lo);
+    } else if (hx < 0x3e300000u) {                 // |x| < 2^-28
+        return add(1.0, x);
+    } else {
+        r = x;
+    }
+    const double t = mul(r, r);
+    const double c =
+        sub(r, mul(t, add(EXP_P1, mul(t, add(EXP_P2, mul(t, add(EXP_P3, mul(t, add(EXP_P4, mul(t, EXP_P5))))))))));
+    if (k == 0) return sub(1.0, sub(dv(mul(r, c), sub(c, 2.0)), r));
+    const double y = sub(1.0, sub(sub(lo, dv(mul(r, c), sub(2.0, c))), hi));
+    if (k >= -1021) return add_expo(y, k);
+    return mul(add_expo(y, k + 1000), TWO_M1000);
+}
+
+TPM_FN double expm1(double x) {
+    const uint32_t hx = hix(x);
+    const bool neg_x = (bits(x) >> 63) != 0;
+    if (hx >= 0x4043687Au) {                       // |x| >= 56 ln2
+        if (hx >= 0x40862E42u) {
+            if (hx >= 0x7ff00000u) {
+                if ((bits(x) & 0x000fffffffffffffull) != 0) return add(x, x);
+                return neg_x ? -1.0 : x;
+            }
+            if (x > EXP_OVER) return from_bits(0x7ff0000000000000ull);  // overflow
+        }
+        if (neg_x) return -1.0;                     // x < -56 ln2: rounds to -1
+    }
+    double hi, lo, c = 0.0;
+    int k = 0;
+    if (hx > 0x3fd62e42u) {                        // |x| > ln2/2
+        if (hx < 0x3FF0A2B2u) {
+            if (!neg_x) { hi = sub(x, LN2_HI); lo = LN2_LO; k = 1; }
+            else { hi = add(x, LN2_HI); lo = -LN2_LO; k = -1; }
+        } else {
+            k = int(add(mul(INV_LN2, x), neg_x ? -0.5 : 0.5));
+            const double t = double(k);
+            hi = sub(x, mul(t, LN2_HI));
+            lo = mul(t, LN2_LO);
+        }
+        x = sub(hi, lo);
+        c = sub(sub(hi, x), lo);
+    } else if (hx < 0x3c900000u) {                 // |x| < 2^-54
+        return x;
+    }
+    const double hfx = mul(0.5, x);
+    const double hxs = mul(x, hfx);
+    const double r1 = add(1.0, mul(hxs, add(EM1_Q1, mul(hxs, add(EM1_Q2, mul(hxs, add(EM1_Q3,
+                                  mul(hxs, add(EM1_Q4, mul(hxs, EM1_Q5))))))))));
+    const double t = sub(3.0, mul(r1, hfx));
+    double e = mul(hxs, dv(sub(r1, t), sub(6.0, mul(x, t))));
+    if (k == 0) return sub(x, sub(mul(x, e), hxs));
+    e = sub(mul(x, sub(e, c)), c);
+    e = sub(e, hxs);
+    if (k == -1) return sub(mul(0.5, sub(x, e)), 0.5);
+    if (k == 1) {
+        if (x < -0.25) return mul(-2.0, sub(e, add(x, 0.5)));
+        return add(1.0, mul(2.0, sub(x, e)));
+    }
+    if (k <= -2 || k > 56) {
+        const double y = sub(1.0, sub(e, x));
+        return sub(add_expo(y, k), 1.0);
+    }
+    if (k < 20) {
+        const double t1 = from_bits(uint64_t(0x3ff00000u - (0x200000u >> k)) << 32);  // 1 - 2^-k
+        const double y = sub(t1, sub(e, x));
+        return add_expo(y, k);
+    }
+    const double t2 = from_bits(uint64_t(uint32_t(0x3ff - k) << 20) << 32);  // 2^-k
+    double y = sub(x, add(e, t2));
+    y = add(y, 1.0);
+    return add_expo(y, k);
+}
+
+TPM_FN double sinh(double x) {
+    const uint32_t ix = hix(x);
+    if (ix >= 0x7ff00000u) return add(x, x);
+    const double h = (bits(x) >> 63) ? -0.5 : 0.5;
+    const double ax = fabs_(x);
+    if (ix < 0x40360000u) {                        // |x| < 22
+        if (ix < 0x3e300000u) return x;            // |x| < 2^-28
+        const double t = expm1(ax);
+        if (ix < 0x3ff00000u) return mul(h, sub(mul(2.0, t), dv(mul(t, t), add(t, 1.0))));
+        return mul(h, add(t, dv(t, add(t, 1.0))));
+    }
+    if (ix < 0x40862E42u) return mul(h, exp(ax));  // |x| < log(DBL_MAX)
+    const double w = exp(mul(0.5, ax));             // up to the overflow threshold
+    return mul(mul(h, w), w);
+}
+
+TPM_FN double cosh(double x) {
+    const uint32_t ix = hix(x);
+    if (ix >= 0x7ff00000u) return mul(x, x);
+    const double ax = fabs_(x);
+    if (ix < 0x3fd62e43u) {                        // |x| < ln2/2
+        const double t = expm1(ax);
+        const double w = add(1.0, t);
+        if (ix < 0x3c800000u) return w;
+        return add(1.0, dv(mul(t, t), add(w, w)));
+    }
+    if (ix < 0x40360000u) {                        // |x| < 22
+        const double t = exp(ax);
+        return add(mul(0.5, t), dv(0.5, t));
+    }
+    if (ix < 0x40862E42u) return mul(0.5, exp(ax));
+    const double w = exp(mul(0.5, ax));
+    return mul(mul(0.5, w), w);
 }
 
 }  // namespace libm

@@ -11,7 +11,8 @@
 //   opd = 1 + delta
 // Multiplication of those cached values reproduces the reference's per-call
 // values exactly, because IEEE operations are deterministic.  sin, cos, tan,
-// asin and atan come from tp_libm.h (the same bits on host and device).
+// asin, atan, exp, sinh and cosh come from tp_libm.h (the same bits on host and
+// device).
 #pragma once
 #include <math_constants.h>
 #include <stdint.h>
@@ -555,9 +556,141 @@ __device__ __forceinline__ void long_rf_map(P6& s, const double* w, double beta)
 __device__ __forceinline__ void strong_thin_gauss(P6& s, const double* w) {
     double dx = s.x - w[stg::XO];
     double dy = s.y - w[stg::YO];
-    double g = w[stg::AMP] * exp(-0.5 * (dx * dx / w[stg::SX2] + dy * dy / w[stg::SY2]));
+    double g = w[stg::AMP] * libm::exp(-0.5 * (dx * dx / w[stg::SX2] + dy * dy / w[stg::SY2]));
     s.px = s.px - g * dx / w[stg::SX2];
     s.py = s.py - g * dy / w[stg::SY2];
+}
+
+// LBend (src/tracking.jl:1076-1170): method-1 edges around the linear
+// combined-function body; G1, G2 depend on delta through p_norm.
+static __device__ __noinline__ void lbend(P6& s, const double* w, const RecHdr& h) {
+    const double kx = w[lb::KX], L = w[lb::L];
+    edge_fringe(s, w[lb::IRHO], w[lb::FX_IN], w[lb::E_IN], w[lb::FC_IN], 1, h.flags & RF_FC_IN_ZERO, false);
+    const double p_norm = 1.0 / (1.0 + s.d);
+    const double G1 = w[lb::G1C] * p_norm;
+    const double G2 = w[lb::NGRD] * p_norm;
+    const double tol = 1.4901161193847656e-08;  // sqrt(eps(Float64))
+    double MHD = 1.0, M12 = L, M21 = 0.0, MVD = 1.0, M34 = L, M43 = 0.0;
+    double arg1 = 0.0, sqrtG1 = 0.0;
+    const bool big1 = fabs(G1) >= tol;
+    if (big1) {
+        if (G1 > 0.0) {
+            sqrtG1 = sqrt(G1);
+            arg1 = L * sqrtG1;
+            MHD = libm::cos(arg1); M12 = libm::sin(arg1) / sqrtG1; M21 = -libm::sin(arg1) * sqrtG1;
+        } else {
+            sqrtG1 = sqrt(-G1);
+            arg1 = L * sqrtG1;
+            MHD = libm::cosh(arg1); M12 = libm::sinh(arg1) / sqrtG1; M21 = libm::sinh(arg1) * sqrtG1;
+        }
+    }
+    if (fabs(G2) >= tol) {
+        if (G2 > 0.0) {
+            const double sq = sqrt(G2), arg2 = L * sq;
+            MVD = libm::cos(arg2); M34 = libm::sin(arg2) / sq; M43 = -libm::sin(arg2) * sq;
+        } else {
+            const double sq = sqrt(-G2), arg2 = L * sq;
+            MVD = libm::cosh(arg2); M34 = libm::sinh(arg2) / sq; M43 = libm::sinh(arg2) * sq;
+        }
+    }
+    const double x = s.x, xpr = s.px * p_norm, y = s.y, ypr = s.py * p_norm;
+    const double dterm = s.d * p_norm - w[lb::BYERR];
+    double x_new = MHD * x + M12 * xpr;
+    double px_new = (M21 * x + MHD * xpr) / p_norm;
+    if (fabs(G1) < tol) {
+        x_new = x_new + dterm * L * L * kx / 2.0;
+        px_new = px_new + dterm * L * kx / p_norm;
+    } else if (G1 > 0.0) {
+        x_new = x_new + dterm * (1.0 - libm::cos(arg1)) * kx / G1;
+        px_new = px_new + dterm * libm::sin(arg1) * kx / (sqrtG1 * p_norm);
+    } else {
+        x_new = x_new + dterm * (1.0 - libm::cosh(arg1)) * kx / G1;
+        px_new = px_new + dterm * libm::sinh(arg1) * kx / (sqrtG1 * p_norm);
+    }
+    const double y_new = MVD * y + M34 * ypr;
+    const double py_new = (M43 * y + MVD * ypr) / p_norm;
+    double z_new = s.z + xpr * xpr * (L + MHD * M12) / 4.0;
+    if (big1) {
+        z_new = z_new + (L - MHD * M12) * (x * x * G1 + dterm * dterm * kx * kx / G1 - 2.0 * x * kx * dterm) / 4.0;
+        z_new = z_new + M12 * M21 * (x * xpr - xpr * dterm * kx / G1) / 2.0;
+        z_new = z_new + (kx * x * M12 + xpr * (1.0 - MHD) * kx / G1 + dterm * (L - M12) * kx * kx / G1);
+    }
+    z_new = z_new + ((L - MVD * M34) * y * y * G2 + ypr * ypr * (L + MVD * M34)) / 4.0;
+    z_new = z_new + M34 * M43 * y * ypr / 2.0;
+    s.x = x_new; s.px = px_new; s.y = y_new; s.py = py_new; s.z = z_new;
+    edge_fringe(s, w[lb::IRHO], w[lb::FX_OUT], w[lb::E_OUT], w[lb::FC_OUT], 1, h.flags & RF_FC_OUT_ZERO, true);
+}
+
+// StrongGaussianBeam (src/tracking.jl:1621-1641): the slice weights and
+// offsets follow the fixed words.
+static __device__ __noinline__ void strong_gauss(P6& s, const double* w) {
+    const int nz = int(w[sgb::NZ]);
+    const double* wt = w + sgb::WORDS;
+    const double factor = w[sgb::FACTOR], sx2 = w[sgb::SX2], sy2 = w[sgb::SY2];
+    double px = s.px, py = s.py;
+    for (int i = 0; i < nz; ++i) {
+        const double dx = s.x - wt[nz + i];
+        const double dy = s.y - wt[2 * nz + i];
+        const double g = wt[i] * libm::exp(-0.5 * (dx * dx / sx2 + dy * dy / sy2));
+        px = px - factor * g * dx / sx2;
+        py = py - factor * g * dy / sy2;
+    }
+    s.px = px;
+    s.py = py;
+}
+
+// LongitudinalRLCWake (src/tracking.jl:1647-1654, wake.jl:27-37).
+__device__ __forceinline__ void rlc_wake(P6& s, const double* w) {
+    const double zc = s.z / C_LIGHT;
+    const double t = isnan(zc) ? zc : (zc > 0.0 ? 0.0 : zc);  // Julia min(z/c, 0)
+    double wf = 0.0;
+    if (!(t > 0.0))
+        wf = w[rlc::A] * (libm::cos(w[rlc::W0P] * t) + libm::sin(w[rlc::W0P] * t) / w[rlc::D2Q0P]) *
+             libm::exp(w[rlc::W0] * t / w[rlc::D2Q0]);
+    s.d = s.d - w[rlc::SCALE] * wf;
+}
+
+// LongitudinalWake (src/tracking.jl:1656-1663, wake.jl:68-91): linear
+// interpolation in the table after the fixed words; with sorted times
+// (h.order = 1) the segment is found by bisection, which selects the same
+// segment as the reference's scan.
+static __device__ __noinline__ void tab_wake(P6& s, const double* w, const RecHdr& h) {
+    const int n = int(w[tw::N]);
+    const double* xs = w + tw::WORDS;
+    const double* ys = xs + n;
+    const double t = s.z / C_LIGHT;
+    double wf = 0.0;
+    if (!(t > w[tw::T1F])) {
+        const double x = t * w[tw::FLIP];
+        if (x <= xs[0]) {
+            const double slope = (ys[1] - ys[0]) / (xs[1] - xs[0]);
+            wf = ys[0] + slope * (x - xs[0]);
+        } else if (x >= xs[n - 1]) {
+            const double slope = (ys[n - 1] - ys[n - 2]) / (xs[n - 1] - xs[n - 2]);
+            wf = ys[n - 1] + slope * (x - xs[n - 1]);
+        } else if (isnan(x)) {
+            wf = ys[n - 1];
+        } else {
+            int i = 1;
+            if (h.order == 1) {  // first i with x < xs[i]; x < xs[n-1] here
+                int lo = 1, hi = n - 1;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (x < xs[mid]) hi = mid; else lo = mid + 1;
+                }
+                i = lo;
+            } else {
+                while (i < n - 1 && !(x < xs[i])) ++i;
+            }
+            if (x < xs[i]) {
+                const double slope = (ys[i] - ys[i - 1]) / (xs[i] - xs[i - 1]);
+                wf = ys[i - 1] + slope * (x - xs[i - 1]);
+            } else {
+                wf = ys[n - 1];
+            }
+        }
+    }
+    s.d = s.d - w[tw::SCALE] * wf;
 }
 
 // Misalignment (src/tracking.jl:60-67): r + t, and the column-major 6x6 product.
@@ -648,6 +781,10 @@ __device__ __forceinline__ bool apply_record(P6& s, const double* rec, const Rec
             break;
         }
         case DK_STRONG_THIN_GAUSS: strong_thin_gauss(s, w); break;
+        case DK_LBEND: lbend(s, w, h); break;
+        case DK_SGB: strong_gauss(s, w); break;
+        case DK_RLC_WAKE: rlc_wake(s, w); break;
+        case DK_TAB_WAKE: tab_wake(s, w, h); break;
         case DK_NAN: set_nan(s); break;
         default: return false;
     }

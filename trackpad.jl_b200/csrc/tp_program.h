@@ -33,7 +33,12 @@ enum DevKind : uint8_t {
     DK_INV_LORENTZ = 15,
     DK_STRONG_THIN_GAUSS = 16,
     DK_NAN = 17,        // maps that return NaN for every particle (SBendSC with L == 0)
-    DK_COUNT = 18
+    DK_LBEND = 18,      // LBend: edges (method 1) + linear combined-function body
+    DK_SGB = 19,        // StrongGaussianBeam: Gaussian kicks of nz slices (arrays in the record)
+    DK_RLC_WAKE = 20,   // LongitudinalRLCWake
+    DK_TAB_WAKE = 21,   // LongitudinalWake: tabulated wake (table in the record)
+    DK_WIGGLER = 22,    // Wiggler (harmonics in the record)
+    DK_COUNT = 23
 };
 
 // Record flags.
@@ -102,6 +107,13 @@ namespace acc { enum { VOLT = 0, E = 1, K = 2, PHIS = 3, SINPHIS = 4, WORDS = 5 
 namespace lrf { enum { ALPHAC = 0, K = 1, H = 2, WORDS = 3 }; }
 namespace lor { enum { A = 0, B = 1, WORDS = 2 }; }  // boost: invcos, tanang; inverse: cosang, sinang
 namespace stg { enum { AMP = 0, SX2 = 1, SY2 = 2, XO = 3, YO = 4, WORDS = 5 }; }
+namespace lb {  // DK_LBEND: body constants, then the SBend edge words
+enum { L = 0, KX = 1, G1C = 2, NGRD = 3, BYERR = 4, IRHO = 5, FX_IN = 6, E_IN = 7, FC_IN = 8,
+       FX_OUT = 9, E_OUT = 10, FC_OUT = 11, WORDS = 12 };
+}
+namespace sgb { enum { FACTOR = 0, SX2 = 1, SY2 = 2, NZ = 3, WORDS = 4 }; }  // then w[nz], xo[nz], yo[nz]
+namespace rlc { enum { SCALE = 0, A = 1, W0P = 2, D2Q0P = 3, W0 = 4, D2Q0 = 5, WORDS = 6 }; }
+namespace tw { enum { SCALE = 0, FLIP = 1, T1F = 2, N = 3, WORDS = 4 }; }  // then times[n], wakes[n]
 
 // Misalignment row as stored on the device (same content as tp_misalign).
 struct MisalignDev {
@@ -113,7 +125,8 @@ struct MisalignDev {
     int32_t pad[2];
 };
 
-// Maximum record length in words (exact bend).
+// Maximum fixed record length in words (exact bend); array-carrying kinds
+// (DK_SGB, DK_TAB_WAKE, DK_WIGGLER) append their arrays after the fixed words.
 constexpr int MAX_REC_WORDS = HDR_WORDS + eb::WORDS;
 
 }  // namespace tp

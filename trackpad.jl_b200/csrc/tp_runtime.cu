@@ -96,6 +96,7 @@ struct DevLattice {
 struct tp_lattice {
     std::vector<tp_elem> elems;
     std::vector<tp_misalign> mis;
+    std::vector<double> aux;           // array fields of the elements (tp_lattice_create_ex)
     std::vector<double> program;       // compiled table, padded to 16 bytes
     std::vector<int32_t> rec_off;      // word offset of each record
     std::vector<double> flops_exact;   // per element, exact drift
@@ -501,30 +502,39 @@ TP_API int tp_last_stats(const tp_ctx* c, tp_stats* out) {
 // ---------------------------------------------------------------------------
 TP_API int tp_lattice_create(const tp_elem* elems, int64_t n, const tp_misalign* mis, int64_t nmis,
                              tp_lattice** out) {
+    return tp_lattice_create_ex(elems, n, mis, nmis, nullptr, 0, out);
+}
+
+TP_API int tp_lattice_create_ex(const tp_elem* elems, int64_t n, const tp_misalign* mis, int64_t nmis,
+                                const double* aux, int64_t naux, tp_lattice** out) {
     if (!out) return set_err(TP_EINVAL, "out is null");
     *out = nullptr;
-    if (n < 0 || nmis < 0) return set_err(TP_EINVAL, "negative size");
+    if (n < 0 || nmis < 0 || naux < 0) return set_err(TP_EINVAL, "negative size");
     if (n > 0 && !elems) return set_err(TP_EINVAL, "elems is null");
     if (nmis > 0 && !mis) return set_err(TP_EINVAL, "mis is null");
+    if (naux > 0 && !aux) return set_err(TP_EINVAL, "aux is null");
     if (n > (int64_t(1) << 24)) return set_err(TP_ERANGE, "lattice longer than 2^24 elements");
+    const AuxView av{aux, naux};
     std::string err;
     for (int64_t i = 0; i < n; ++i) {
-        int st = validate_elem(elems[i], i, nmis, &err);
+        int st = validate_elem(elems[i], i, nmis, &err, av);
         if (st != TP_OK) return set_err(st, err);
     }
     tp_lattice* L = new (std::nothrow) tp_lattice();
     if (!L) return set_err(TP_ENOMEM, "host allocation failed");
     L->elems.assign(elems, elems + n);
     if (nmis > 0) L->mis.assign(mis, mis + nmis);
+    if (naux > 0) L->aux.assign(aux, aux + naux);
+    const AuxView lav{L->aux.data(), int64_t(L->aux.size())};
     L->rec_off.resize(size_t(n));
     L->flops_exact.resize(size_t(n));
     L->flops_lin.resize(size_t(n));
     for (int64_t i = 0; i < n; ++i) {
         L->rec_off[size_t(i)] = int32_t(L->program.size());
-        compile_record(elems[i], &L->program);
+        compile_record(elems[i], &L->program, lav);
         const tp_misalign* m = elems[i].misalign_index >= 0 ? &mis[elems[i].misalign_index] : nullptr;
-        L->flops_exact[size_t(i)] = elem_flops(elems[i], m, true);
-        L->flops_lin[size_t(i)] = elem_flops(elems[i], m, false);
+        L->flops_exact[size_t(i)] = elem_flops(elems[i], m, true, lav);
+        L->flops_lin[size_t(i)] = elem_flops(elems[i], m, false, lav);
     }
     if (L->program.size() > (size_t(1) << 30)) {
         delete L;
@@ -573,7 +583,7 @@ TP_API int tp_lattice_set_schedule(tp_lattice* L, const int32_t* fields, int32_t
         L->program.clear();
         for (size_t i = 0; i < L->elems.size(); ++i) {
             L->rec_off[i] = int32_t(L->program.size());
-            compile_record(L->elems[i], &L->program);
+            compile_record(L->elems[i], &L->program, AuxView{L->aux.data(), int64_t(L->aux.size())});
         }
         while (L->program.size() % 2) L->program.push_back(0.0);
         L->has_sched = false;
@@ -596,7 +606,7 @@ TP_API int tp_lattice_set_schedule(tp_lattice* L, const int32_t* fields, int32_t
     int32_t stride = 0;
     for (int32_t e : sched_elems) {
         slot[size_t(e)] = stride;
-        stride += record_words(L->elems[size_t(e)]);
+        stride += record_words(L->elems[size_t(e)], AuxView{L->aux.data(), int64_t(L->aux.size())});
     }
     std::vector<double> table;
     table.reserve(size_t(stride) * size_t(nturns));
@@ -606,19 +616,21 @@ TP_API int tp_lattice_set_schedule(tp_lattice* L, const int32_t* fields, int32_t
             tp_elem x = L->elems[size_t(e)];
             for (int32_t j = 0; j < nfields; ++j)
                 if (fields[2 * j] == e) apply_field(&x, fields[2 * j + 1], values[int64_t(t) * nfields + j]);
-            int st = validate_elem(x, e, int64_t(L->mis.size()), &err);
+            const AuxView lav{L->aux.data(), int64_t(L->aux.size())};
+            int st = validate_elem(x, e, int64_t(L->mis.size()), &err, lav);
             if (st != TP_OK) return set_err(st, err);
             size_t before = table.size();
-            compile_record(x, &table);
-            if (int32_t(table.size() - before) != record_words(L->elems[size_t(e)]))
+            compile_record(x, &table, lav);
+            if (int32_t(table.size() - before) != record_words(L->elems[size_t(e)], lav))
                 return set_err(TP_EINVAL, "schedule changes the record layout of an element");
         }
     }
     L->program.clear();
     for (int64_t i = 0; i < ne; ++i) {
         L->rec_off[size_t(i)] = int32_t(L->program.size());
-        if (slot[size_t(i)] >= 0) scheduled_stub(L->elems[size_t(i)], slot[size_t(i)], &L->program);
-        else compile_record(L->elems[size_t(i)], &L->program);
+        const AuxView lav{L->aux.data(), int64_t(L->aux.size())};
+        if (slot[size_t(i)] >= 0) scheduled_stub(L->elems[size_t(i)], slot[size_t(i)], &L->program, lav);
+        else compile_record(L->elems[size_t(i)], &L->program, lav);
     }
     while (L->program.size() % 2) L->program.push_back(0.0);
     L->sfields.assign(fields, fields + 2 * nfields);

@@ -58,10 +58,11 @@ class AbstractElement:
         """Dict of tp_elem fields (reference names)."""
         raise NotImplementedError
 
-    def pack(self):
+    def pack(self, aux=None):
+        """The tp_elem record; array fields are appended to `aux`."""
         d = self._fields()
         d["kind"] = self.kind
-        return _abi.elem_from_dict(d)
+        return _abi.elem_from_dict(d, aux)
 
     def misalignment(self):
         m = _abi.TpMisalign()
@@ -453,7 +454,93 @@ class StrongThinGaussianBeam(AbstractElement):
         return 0.0
 
 
+class LBend(AbstractElement):
+    """src/elements/SCelements.jl:346-383 (linear combined-function bend, method-1 edges)."""
+    kind = "LBEND"
+    _misalignable = True
+
+    def __init__(self, L, angle, e1=0.0, e2=0.0, *, name="LBEND", K=0.0, by_error=0.0, fint1=0.0, fint2=0.0,
+                 full_gap=0.0, t1=None, t2=None, r1=None, r2=None, r_apertures=None, e_apertures=None):
+        self.name = name
+        self.L, self.angle, self.e1, self.e2 = float(L), float(angle), float(e1), float(e2)
+        self.K, self.by_error = float(K), float(by_error)
+        self.fint1, self.fint2, self.full_gap = float(fint1), float(fint2), float(full_gap)
+        self._misalign_init(t1, t2, r1, r2)
+
+    def _fields(self):
+        return {"L": self.L, "angle": self.angle, "e1": self.e1, "e2": self.e2, "fint1": self.fint1,
+                "fint2": self.fint2, "gap": self.full_gap, "param": [self.K, self.by_error] + [0.0] * 6}
+
+
+class StrongGaussianBeam(AbstractElement):
+    """src/elements/beambeam.jl:83-121: Gaussian kicks of nzslice slices."""
+    kind = "STRONG_GAUSSIAN_BEAM"
+
+    def __init__(self, charge, mass, atomnum, num_particle, total_energy, beamsize, *, name="STRONGGAUSSIANBEAM",
+                 nzslice=1, zslice_center=None, zslice_npar=None, xoffsets=None, yoffsets=None):
+        self.name = name
+        self.charge, self.mass, self.atomnum = float(charge), float(mass), float(atomnum)
+        self.num_particle = int(num_particle)
+        self.total_energy = float(total_energy)
+        self.beamsize = [float(beamsize[0]), float(beamsize[1])]
+        self.nzslice = int(nzslice)
+        n = self.nzslice
+        self.zslice_center = ([-1.0 + 2.0 * i / (n - 1) for i in range(n)] if n > 1 else [-1.0] * n) \
+            if zslice_center is None else [float(v) for v in zslice_center]
+        self.zslice_npar = [1.0 / max(n, 1)] * n if zslice_npar is None else [float(v) for v in zslice_npar]
+        self.xoffsets = [0.0] * n if xoffsets is None else [float(v) for v in xoffsets]
+        self.yoffsets = [0.0] * n if yoffsets is None else [float(v) for v in yoffsets]
+
+    def _fields(self):
+        n = max(self.nzslice, 0)
+        # the pass reads slice i's weight and offsets, or 1/nzslice and 0 past the arrays' ends
+        w = [self.zslice_npar[i] if i < len(self.zslice_npar) else 1.0 / n for i in range(n)]
+        xo = [self.xoffsets[i] if i < len(self.xoffsets) else 0.0 for i in range(n)]
+        yo = [self.yoffsets[i] if i < len(self.yoffsets) else 0.0 for i in range(n)]
+        return {"param": [self.charge, self.total_energy, self.beamsize[0], self.beamsize[1]] + [0.0] * 4,
+                "aux": w + xo + yo}
+
+    def get_length(self):
+        return 0.0
+
+
+class LongitudinalRLCWake(AbstractElement):
+    """src/elements/wake.jl:6-18: resonator wake, a function of each particle's z."""
+    kind = "LONGITUDINAL_RLC_WAKE"
+
+    def __init__(self, *, name="LONGITUDINALRLCWAKE", freq=1.0e9, Rshunt=1.0e6, Q0=1.0, scale=0.0):
+        self.name = name
+        self.freq, self.Rshunt, self.Q0, self.scale = float(freq), float(Rshunt), float(Q0), float(scale)
+
+    def _fields(self):
+        return {"param": [self.freq, self.Rshunt, self.Q0, self.scale] + [0.0] * 4}
+
+    def get_length(self):
+        return 0.0
+
+
+class LongitudinalWake(AbstractElement):
+    """src/elements/wake.jl:44-58: tabulated wake, interpolated at each particle's z."""
+    kind = "LONGITUDINAL_WAKE"
+
+    def __init__(self, times, wakefields, *, name="LONGITUDINALWAKE", fliphalf=-1.0, scale=0.0):
+        if len(times) != len(wakefields):
+            raise ValueError("times and wakefields must have the same length")
+        if len(times) < 2:
+            raise ValueError("LongitudinalWake requires at least two samples")
+        self.name = name
+        self.times = [float(v) for v in times]
+        self.wakefields = [float(v) for v in wakefields]
+        self.fliphalf, self.scale = float(fliphalf), float(scale)
+
+    def _fields(self):
+        return {"param": [self.fliphalf, self.scale] + [0.0] * 6, "aux": self.times + self.wakefields}
+
+    def get_length(self):
+        return 0.0
+
+
 ELEMENT_TYPES = [Marker, Drift, Quadrupole, Sextupole, Octupole, ThinMultipole, SBend, ExactSBend, RFCavity,
                  Solenoid, Corrector, Translation, YRotation, CrabCavity, AccelCavity, LongitudinalRFMap,
                  LorentzBoost, InvLorentzBoost, SpaceCharge, DriftSC, QuadrupoleSC, SextupoleSC, OctupoleSC,
-                 SBendSC, StrongThinGaussianBeam]
+                 SBendSC, StrongThinGaussianBeam, LBend, StrongGaussianBeam, LongitudinalRLCWake, LongitudinalWake]

@@ -199,26 +199,30 @@ class Lattice:
         return [e.base if isinstance(e, TimeVaryingElement) else e for e in self.elements]
 
     def pack(self):
+        """(tp_elem array, n, misalignment array, nmis, aux float64 array)."""
         if getattr(self, "_records", None) is not None:
-            arr = _abi.elem_array(self._records)
-            return arr, len(self._records), (_abi.TpMisalign * 1)(), 0
+            arr, aux = _abi.elem_array_aux(self._records)
+            return arr, len(self._records), (_abi.TpMisalign * 1)(), 0, np.asarray(aux, dtype=np.float64)
         elems = self._static_elements()
         arr = (_abi.TpElem * max(len(elems), 1))()
         mis = []
+        aux = []
         for i, e in enumerate(elems):
-            arr[i] = e.pack()
+            arr[i] = e.pack(aux)
             if e.has_misalignment():
                 arr[i].misalign_index = len(mis)
                 mis.append(e.misalignment())
         marr = (_abi.TpMisalign * max(len(mis), 1))(*mis)
-        return arr, len(elems), marr, len(mis)
+        return arr, len(elems), marr, len(mis), np.asarray(aux, dtype=np.float64)
 
     @property
     def handle(self):
         if self._handle is None:
-            arr, n, marr, nm = self.pack()
+            arr, n, marr, nm, aux = self.pack()
             h = C.c_void_p()
-            _abi.check(_abi.lib().tp_lattice_create(arr, n, marr if nm else None, nm, C.byref(h)), "tp_lattice_create")
+            _abi.check(_abi.lib().tp_lattice_create_ex(arr, n, marr if nm else None, nm,
+                                                       aux.ctypes.data_as(C.c_void_p) if len(aux) else None,
+                                                       len(aux), C.byref(h)), "tp_lattice_create_ex")
             self._handle = h
         return self._handle
 
