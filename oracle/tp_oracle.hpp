@@ -898,6 +898,237 @@ inline V6<T> pass_tab_wake(const Elem<T>& e, const V6<T>& r) {
 }
 
 // ---------------------------------------------------------------------------
+// Wiggler: src/tracking.jl:1224-1529.  aux = NHharm, NVharm, rad, By[6 NH],
+// Bx[6 NV]; harmonic i of By is (_, HCw, kx/kw, ky/kw, kz/kw, tz).
+// param = lw, Bmax, energy; num_int_steps = Nsteps.
+// ---------------------------------------------------------------------------
+template <class T>
+inline T sinc_taylor(T x) {  // _sinc_taylor :1226-1229
+    T x2 = x * x;
+    return T(1.0) - x2 / T(6.0) * (T(1.0) - x2 / T(20.0) * (T(1.0) - x2 / T(42.0) * (T(1.0) - x2 / T(72.0))));
+}
+
+template <class T>
+struct Wig {
+    const Elem<T>* e;
+    int nh, nv;
+    const double* by;
+    const double* bx;
+    T lw, bmax;
+};
+
+template <class T>
+inline Wig<T> wig_of(const Elem<T>& e) {
+    Wig<T> w;
+    w.e = &e;
+    w.nh = int(e.aux[0]);
+    w.nv = int(e.aux[1]);
+    w.by = e.aux + 3;
+    w.bx = e.aux + 3 + 6 * w.nh;
+    w.lw = e.param[0];
+    w.bmax = e.param[1];
+    return w;
+}
+
+// _wig_ax_axpy :1231-1280
+template <class T>
+inline void wig_ax_axpy(const Wig<T>& w, T x, T y, T Zw, T Aw, T Po, T& ax, T& axpy) {
+    using std::abs;
+    T kw = T(TWO_PI) / w.lw;
+    ax = T(0.0);
+    axpy = T(0.0);
+    for (int i = 0; i < w.nh; ++i) {
+        const double* b = w.by + 6 * i;
+        T HCw = T(b[1]) * Aw / Po;
+        T kx = T(b[2]) * kw, ky = T(b[3]) * kw, kz = T(b[4]) * kw, tz = T(b[5]);
+        T cx = cos(kx * x);
+        T chy = cosh(ky * y);
+        T sz = sin(kz * Zw + tz);
+        ax = ax + HCw * (kw / kz) * cx * chy * sz;
+        T shy = sinh(ky * y);
+        T sxkx = value_of(abs(kx / kw)) > 1e-6 ? sin(kx * x) / kx : x * sinc_taylor(kx * x);
+        axpy = axpy + HCw * (kw / kz) * ky * sxkx * shy * sz;
+    }
+    for (int i = 0; i < w.nv; ++i) {
+        const double* b = w.bx + 6 * i;
+        T VCw = T(b[1]) * Aw / Po;
+        T kx = T(b[2]) * kw, ky = T(b[3]) * kw, kz = T(b[4]) * kw, tz = T(b[5]);
+        T shx = sinh(kx * x);
+        T sy = sin(ky * y);
+        T sz = sin(kz * Zw + tz);
+        ax = ax + VCw * (kw / kz) * (ky / kx) * shx * sy * sz;
+        T chx = cosh(kx * x);
+        T cy = cos(ky * y);
+        axpy = axpy + VCw * (kw / kz) * ((ky / kx) * (ky / kx)) * chx * cy * sz;
+    }
+}
+
+// _wig_ay_aypx :1282-1331
+template <class T>
+inline void wig_ay_aypx(const Wig<T>& w, T x, T y, T Zw, T Aw, T Po, T& ay, T& aypx) {
+    using std::abs;
+    T kw = T(TWO_PI) / w.lw;
+    ay = T(0.0);
+    aypx = T(0.0);
+    for (int i = 0; i < w.nh; ++i) {
+        const double* b = w.by + 6 * i;
+        T HCw = T(b[1]) * Aw / Po;
+        T kx = T(b[2]) * kw, ky = T(b[3]) * kw, kz = T(b[4]) * kw, tz = T(b[5]);
+        T sx = sin(kx * x);
+        T shy = sinh(ky * y);
+        T sz = sin(kz * Zw + tz);
+        ay = ay + HCw * (kw / kz) * (kx / ky) * sx * shy * sz;
+        T cx = cos(kx * x);
+        T chy = cosh(ky * y);
+        aypx = aypx + HCw * (kw / kz) * ((kx / ky) * (kx / ky)) * cx * chy * sz;
+    }
+    for (int i = 0; i < w.nv; ++i) {
+        const double* b = w.bx + 6 * i;
+        T VCw = T(b[1]) * Aw / Po;
+        T kx = T(b[2]) * kw, ky = T(b[3]) * kw, kz = T(b[4]) * kw, tz = T(b[5]);
+        T chx = cosh(kx * x);
+        T cy = cos(ky * y);
+        T sz = sin(kz * Zw + tz);
+        ay = ay + VCw * (kw / kz) * chx * cy * sz;
+        T shx = sinh(kx * x);
+        T syky = value_of(abs(ky / kw)) > 1e-6 ? sin(ky * y) / ky : y * sinc_taylor(ky * y);
+        aypx = aypx + VCw * (kw / kz) * kx * shx * syky * sz;
+    }
+}
+
+// _wig_map_2nd :1333-1378 (Zw is advanced in place)
+template <class T>
+inline V6<T> wig_map_2nd(const Wig<T>& w, const V6<T>& r, T dl, T& Zw, T Aw, T Po) {
+    T delta = r[5];
+    T inv1pd = T(1.0) / (T(1.0) + delta);
+    T dld = dl * inv1pd;
+    T dl2 = dl / T(2.0);
+    T dl2d = dl2 * inv1pd;
+    Zw = Zw + dl2;
+    T x = r[0], px = r[1], y = r[2], py = r[3], z = r[4];
+    T a, ap;
+    wig_ay_aypx(w, x, y, Zw, Aw, Po, a, ap);
+    px = px - ap;
+    py = py - a;
+    y = y + dl2d * py;
+    z = z + (dl2d / T(2.0)) * (py * py) * inv1pd;
+    wig_ay_aypx(w, x, y, Zw, Aw, Po, a, ap);
+    px = px + ap;
+    py = py + a;
+    wig_ax_axpy(w, x, y, Zw, Aw, Po, a, ap);
+    px = px - a;
+    py = py - ap;
+    x = x + dld * px;
+    z = z + (dld / T(2.0)) * (px * px) * inv1pd;
+    wig_ax_axpy(w, x, y, Zw, Aw, Po, a, ap);
+    px = px + a;
+    py = py + ap;
+    wig_ay_aypx(w, x, y, Zw, Aw, Po, a, ap);
+    px = px - ap;
+    py = py - a;
+    y = y + dl2d * py;
+    z = z + (dl2d / T(2.0)) * (py * py) * inv1pd;
+    wig_ay_aypx(w, x, y, Zw, Aw, Po, a, ap);
+    px = px + ap;
+    py = py + a;
+    Zw = Zw + dl2;
+    return V6<T>{{x, px, y, py, z, delta}};
+}
+
+// _wig_B :1400-1449 (the longitudinal field is computed and unused, as there)
+template <class T>
+inline void wig_B(const Wig<T>& w, T x, T y, T Zw, T& Bxv, T& Byv) {
+    T kw = T(TWO_PI) / w.lw;
+    T PB0 = w.bmax;
+    Bxv = T(0.0);
+    Byv = T(0.0);
+    T Bzv = T(0.0);
+    for (int i = 0; i < w.nh; ++i) {
+        const double* b = w.by + 6 * i;
+        T HCw = T(b[1]);
+        T kx = T(b[2]) * kw, ky = T(b[3]) * kw, kz = T(b[4]) * kw, tz = T(b[5]);
+        T sx = sin(kx * x), cx = cos(kx * x), chy = cosh(ky * y), shy = sinh(ky * y);
+        T cz = cos(kz * Zw + tz), sz = sin(kz * Zw + tz);
+        Bxv = Bxv + PB0 * HCw * (kx / ky) * sx * shy * cz;
+        Byv = Byv - PB0 * HCw * cx * chy * cz;
+        Bzv = Bzv + PB0 * HCw * (kz / ky) * cx * shy * sz;
+    }
+    for (int i = 0; i < w.nv; ++i) {
+        const double* b = w.bx + 6 * i;
+        T VCw = T(b[1]);
+        T kx = T(b[2]) * kw, ky = T(b[3]) * kw, kz = T(b[4]) * kw, tz = T(b[5]);
+        T shx = sinh(kx * x), chx = cosh(kx * x), sy = sin(ky * y), cy = cos(ky * y);
+        T cz = cos(kz * Zw + tz), sz = sin(kz * Zw + tz);
+        Bxv = Bxv + PB0 * VCw * chx * cy * cz;
+        Byv = Byv - PB0 * VCw * (ky / kx) * shx * sy * cz;
+        Bzv = Bzv - PB0 * VCw * (kz / kx) * cy * shx * sz;
+    }
+    (void)Bzv;
+}
+
+// _wig_radiation_kicks :1451-1463
+template <class T>
+inline V6<T> wig_rad_kick(const V6<T>& r, T Bxv, T Byv, T Po, T srCoef, T dl) {
+    T B2 = Bxv * Bxv + Byv * Byv;
+    if (value_of(B2) == 0.0) return r;
+    T H = Po * T(M_ELECTRON) / T(C_LIGHT);
+    T irho2 = B2 / (H * H);
+    T dFactor = (T(1.0) + r[5]) * (T(1.0) + r[5]);
+    T dDelta = -srCoef * dFactor * irho2 * dl;
+    T scale = T(1.0) + dDelta;
+    return V6<T>{{r[0], r[1] * scale, r[2], r[3] * scale, r[4], r[5] + dDelta}};
+}
+
+template <class T>
+inline V6<T> wig_rad_block(const Wig<T>& w, V6<T> r, T Zw, T Aw, T Po, T srCoef, T SL) {
+    T ax, axpy, ay, aypx, Bxv, Byv;
+    wig_ax_axpy(w, r[0], r[2], Zw, Aw, Po, ax, axpy);
+    wig_ay_aypx(w, r[0], r[2], Zw, Aw, Po, ay, aypx);
+    r = V6<T>{{r[0], r[1] - ax, r[2], r[3] - ay, r[4], r[5]}};
+    wig_B(w, r[0], r[2], Zw, Bxv, Byv);
+    r = wig_rad_kick(r, Bxv, Byv, Po, srCoef, SL);
+    return V6<T>{{r[0], r[1] + ax, r[2], r[3] + ay, r[4], r[5]}};
+}
+
+// _wig_pass_4th :1380-1398 and _wig_pass_4th_rad :1465-1503; pass!(::Wiggler) :1509-1525
+template <class T>
+inline V6<T> pass_wiggler(const Elem<T>& e, V6<T> r) {
+    using std::sqrt;
+    r = entrance(e, r);
+    Wig<T> w = wig_of(e);
+    const int rad = int(e.aux[2]);
+    const int PN = e.num_int_steps;
+    const long Nw = long(std::nearbyint(value_of(e.L) / value_of(w.lw)));  // round(Int, L/lw): half to even
+    const long Nstep = long(PN) * std::max(1L, Nw);
+    T dl = w.lw / T(double(PN));
+    T dl1 = dl * T(1.3512071919596573);
+    T dl0 = dl * T(-1.7024143839193146);
+    T energy = e.param[2];
+    T Aw = T(1e-9) * T(C_LIGHT) / (T(M_ELECTRON) * T(1e-9)) / T(TWO_PI) * w.lw * w.bmax;
+    T Zw = T(0.0);
+    if (rad == 1) {
+        T gamma = energy / T(M_ELECTRON);
+        T Po = sqrt(gamma * gamma - T(1.0));
+        T srCoef = T(2.0 / 3.0) * T(2.8179403205e-15) * (gamma * gamma * gamma);
+        r = wig_rad_block(w, r, Zw, Aw, Po, srCoef, dl);
+        for (long s = 0; s < Nstep; ++s) {
+            r = wig_map_2nd(w, r, dl1, Zw, Aw, Po);
+            r = wig_map_2nd(w, r, dl0, Zw, Aw, Po);
+            r = wig_map_2nd(w, r, dl1, Zw, Aw, Po);
+            r = wig_rad_block(w, r, Zw, Aw, Po, srCoef, dl);
+        }
+    } else {
+        T Po = sqrt((energy / T(M_ELECTRON)) * (energy / T(M_ELECTRON)) - T(1.0));
+        for (long s = 0; s < Nstep; ++s) {
+            r = wig_map_2nd(w, r, dl1, Zw, Aw, Po);
+            r = wig_map_2nd(w, r, dl0, Zw, Aw, Po);
+            r = wig_map_2nd(w, r, dl1, Zw, Aw, Po);
+        }
+    }
+    return exit_(e, r);
+}
+
+// ---------------------------------------------------------------------------
 // pass! dispatch (multiple dispatch in the reference)
 // ---------------------------------------------------------------------------
 template <class T>
@@ -930,6 +1161,7 @@ inline V6<T> pass(const Elem<T>& e, const V6<T>& r, T beti, bool exact) {
         case TP_STRONG_GAUSSIAN_BEAM: return pass_strong_gaussian(e, r);
         case TP_LONGITUDINAL_RLC_WAKE: return pass_rlc_wake(e, r);
         case TP_LONGITUDINAL_WAKE: return pass_tab_wake(e, r);
+        case TP_WIGGLER: return pass_wiggler(e, r);
         default: return nan6<T>();
     }
 }

@@ -290,6 +290,170 @@ def interpolate(x, xs, ys):  # _linear_interpolate, wake.jl:68-84
     return ys[-1]
 
 
+def Wiggler(L, lw=0.0, Bmax=0.0, Nsteps=10, By=(1, 1, 0, 1, 1, 0), Bx=(), energy=1.0e9, rad=0):  # wiggler.jl:23-44
+    return elem("WIGGLER", L=L, num_int_steps=Nsteps, param=[lw, Bmax, energy] + [0.0] * 5,
+                aux=[float(len(By) // 6), float(len(Bx) // 6), float(rad)] + [float(v) for v in By]
+                + [float(v) for v in Bx])
+
+
+def sinc_taylor(x):  # tracking.jl:1226-1229
+    x2 = x * x
+    return 1.0 - x2 / 6 * (1.0 - x2 / 20 * (1.0 - x2 / 42 * (1.0 - x2 / 72)))
+
+
+def wig_harmonics(e):
+    a = e["aux"]
+    nh, nv = int(a[0]), int(a[1])
+    by = [a[3 + 6 * i: 9 + 6 * i] for i in range(nh)]
+    bx = [a[3 + 6 * nh + 6 * i: 9 + 6 * nh + 6 * i] for i in range(nv)]
+    return by, bx
+
+
+def wig_ax_axpy(e, x, y, Zw, Aw, Po):  # tracking.jl:1231-1280
+    by, bx = wig_harmonics(e)
+    kw = TWO_PI / e["param"][0]
+    ax = axpy = 0.0
+    for h in by:
+        HCw = h[1] * Aw / Po
+        kx, ky, kz, tz = h[2] * kw, h[3] * kw, h[4] * kw, h[5]
+        cx, chy, sz = fm.cos(kx * x), fm.cosh(ky * y), fm.sin(kz * Zw + tz)
+        ax += HCw * (kw / kz) * cx * chy * sz
+        shy = fm.sinh(ky * y)
+        sxkx = fm.sin(kx * x) / kx if abs(kx / kw) > 1e-6 else x * sinc_taylor(kx * x)
+        axpy += HCw * (kw / kz) * ky * sxkx * shy * sz
+    for h in bx:
+        VCw = h[1] * Aw / Po
+        kx, ky, kz, tz = h[2] * kw, h[3] * kw, h[4] * kw, h[5]
+        shx, sy, sz = fm.sinh(kx * x), fm.sin(ky * y), fm.sin(kz * Zw + tz)
+        ax += VCw * (kw / kz) * (ky / kx) * shx * sy * sz
+        chx, cy = fm.cosh(kx * x), fm.cos(ky * y)
+        axpy += VCw * (kw / kz) * ((ky / kx) * (ky / kx)) * chx * cy * sz
+    return ax, axpy
+
+
+def wig_ay_aypx(e, x, y, Zw, Aw, Po):  # tracking.jl:1282-1331
+    by, bx = wig_harmonics(e)
+    kw = TWO_PI / e["param"][0]
+    ay = aypx = 0.0
+    for h in by:
+        HCw = h[1] * Aw / Po
+        kx, ky, kz, tz = h[2] * kw, h[3] * kw, h[4] * kw, h[5]
+        sx, shy, sz = fm.sin(kx * x), fm.sinh(ky * y), fm.sin(kz * Zw + tz)
+        ay += HCw * (kw / kz) * (kx / ky) * sx * shy * sz
+        cx, chy = fm.cos(kx * x), fm.cosh(ky * y)
+        aypx += HCw * (kw / kz) * ((kx / ky) * (kx / ky)) * cx * chy * sz
+    for h in bx:
+        VCw = h[1] * Aw / Po
+        kx, ky, kz, tz = h[2] * kw, h[3] * kw, h[4] * kw, h[5]
+        chx, cy, sz = fm.cosh(kx * x), fm.cos(ky * y), fm.sin(kz * Zw + tz)
+        ay += VCw * (kw / kz) * chx * cy * sz
+        shx = fm.sinh(kx * x)
+        syky = fm.sin(ky * y) / ky if abs(ky / kw) > 1e-6 else y * sinc_taylor(ky * y)
+        aypx += VCw * (kw / kz) * kx * shx * syky * sz
+    return ay, aypx
+
+
+def wig_map_2nd(e, r, dl, Zw, Aw, Po):  # tracking.jl:1333-1378
+    delta = r[5]
+    inv1pd = 1.0 / (1.0 + delta)
+    dld = dl * inv1pd
+    dl2 = dl / 2
+    dl2d = dl2 * inv1pd
+    Zw += dl2
+    x, px, y, py, z = r[0], r[1], r[2], r[3], r[4]
+    ay, aypx = wig_ay_aypx(e, x, y, Zw, Aw, Po)
+    px -= aypx
+    py -= ay
+    y += dl2d * py
+    z += (dl2d / 2) * (py * py) * inv1pd
+    ay, aypx = wig_ay_aypx(e, x, y, Zw, Aw, Po)
+    px += aypx
+    py += ay
+    ax, axpy = wig_ax_axpy(e, x, y, Zw, Aw, Po)
+    px -= ax
+    py -= axpy
+    x += dld * px
+    z += (dld / 2) * (px * px) * inv1pd
+    ax, axpy = wig_ax_axpy(e, x, y, Zw, Aw, Po)
+    px += ax
+    py += axpy
+    ay, aypx = wig_ay_aypx(e, x, y, Zw, Aw, Po)
+    px -= aypx
+    py -= ay
+    y += dl2d * py
+    z += (dl2d / 2) * (py * py) * inv1pd
+    ay, aypx = wig_ay_aypx(e, x, y, Zw, Aw, Po)
+    px += aypx
+    py += ay
+    Zw += dl2
+    return (x, px, y, py, z, delta), Zw
+
+
+def wig_B(e, x, y, Zw):  # tracking.jl:1400-1449 (Bz unused)
+    by, bx = wig_harmonics(e)
+    kw = TWO_PI / e["param"][0]
+    PB0 = e["param"][1]
+    Bxv = Byv = 0.0
+    for h in by:
+        HCw = h[1]
+        kx, ky, kz, tz = h[2] * kw, h[3] * kw, h[4] * kw, h[5]
+        sx, cx, chy, shy = fm.sin(kx * x), fm.cos(kx * x), fm.cosh(ky * y), fm.sinh(ky * y)
+        cz = fm.cos(kz * Zw + tz)
+        Bxv += PB0 * HCw * (kx / ky) * sx * shy * cz
+        Byv -= PB0 * HCw * cx * chy * cz
+    for h in bx:
+        VCw = h[1]
+        kx, ky, kz, tz = h[2] * kw, h[3] * kw, h[4] * kw, h[5]
+        shx, chx, sy, cy = fm.sinh(kx * x), fm.cosh(kx * x), fm.sin(ky * y), fm.cos(ky * y)
+        cz = fm.cos(kz * Zw + tz)
+        Bxv += PB0 * VCw * chx * cy * cz
+        Byv -= PB0 * VCw * (ky / kx) * shx * sy * cz
+    return Bxv, Byv
+
+
+def wig_rad_block(e, r, Zw, Aw, Po, srCoef, SL):  # tracking.jl:1451-1463, 1477-1483
+    ax, _ = wig_ax_axpy(e, r[0], r[2], Zw, Aw, Po)
+    ay, _ = wig_ay_aypx(e, r[0], r[2], Zw, Aw, Po)
+    r = (r[0], r[1] - ax, r[2], r[3] - ay, r[4], r[5])
+    Bxv, Byv = wig_B(e, r[0], r[2], Zw)
+    B2 = Bxv * Bxv + Byv * Byv
+    if B2 != 0.0:
+        H = Po * M_ELECTRON / C_LIGHT
+        irho2 = B2 / (H * H)
+        dFactor = (1.0 + r[5]) * (1.0 + r[5])
+        dDelta = -srCoef * dFactor * irho2 * SL
+        sc = 1.0 + dDelta
+        r = (r[0], r[1] * sc, r[2], r[3] * sc, r[4], r[5] + dDelta)
+    return (r[0], r[1] + ax, r[2], r[3] + ay, r[4], r[5])
+
+
+def wiggler(e, r):  # tracking.jl:1380-1398, 1465-1503, 1509-1525
+    lw, Bmax, energy = e["param"][:3]
+    rad = int(e["aux"][2])
+    PN = e["num_int_steps"]
+    Nw = round(e["L"] / lw)  # Python round: half to even, as Julia's round(Int, x)
+    Nstep = PN * max(1, Nw)
+    dl = lw / PN
+    dl1, dl0 = dl * 1.3512071919596573, dl * -1.7024143839193146
+    Aw = 1e-9 * C_LIGHT / (M_ELECTRON * 1e-9) / TWO_PI * lw * Bmax
+    Zw = 0.0
+    if rad == 1:
+        gamma = energy / M_ELECTRON
+        Po = math.sqrt(gamma * gamma - 1.0)
+        srCoef = (2.0 / 3.0) * 2.8179403205e-15 * (gamma * gamma * gamma)
+        r = wig_rad_block(e, r, Zw, Aw, Po, srCoef, dl)
+        for _ in range(Nstep):
+            for d in (dl1, dl0, dl1):
+                r, Zw = wig_map_2nd(e, r, d, Zw, Aw, Po)
+            r = wig_rad_block(e, r, Zw, Aw, Po, srCoef, dl)
+        return r
+    Po = math.sqrt((energy / M_ELECTRON) * (energy / M_ELECTRON) - 1.0)
+    for _ in range(Nstep):
+        for d in (dl1, dl0, dl1):
+            r, Zw = wig_map_2nd(e, r, d, Zw, Aw, Po)
+    return r
+
+
 def lost_check(r):  # tracking.jl:49-52
     return (math.isnan(r[0]) or abs(r[0]) > COORD_LIMIT or abs(r[2]) > COORD_LIMIT
             or abs(r[1]) > ANGLE_LIMIT or abs(r[3]) > ANGLE_LIMIT)
@@ -642,6 +806,8 @@ def apply_pass(e, r, beti):
         wf = 0.0 if t > 0.0 else rsh * w0 / q0 * (fm.cos(w0p * t) + fm.sin(w0p * t) / (2 * q0p)) * \
             fm.exp(w0 * t / (2 * q0))
         return (r[0], r[1], r[2], r[3], r[4], r[5] - scale * wf)
+    if kind == "WIGGLER":
+        return wiggler(e, r)
     if kind == "LONGITUDINAL_WAKE":  # tracking.jl:1656-1663, wake.jl:86-91
         flip, scale = e["param"][:2]
         if scale == 0.0:
@@ -753,6 +919,10 @@ def extra_cases(energy):
         ("LongitudinalRLCWake", [LongitudinalRLCWake(1.2e9, 2.0e5, 3.5, 2e-19)]),
         ("LongitudinalWake", [LongitudinalWake([0.0, 2e-12, 5e-12, 1e-11, 3e-11],
                                                [1e13, 6e12, 2e12, -1e12, 0.0], fliphalf=-3.0, scale=1e-19)]),
+        ("Wiggler", [Wiggler(1.0, lw=0.1, Bmax=1.2, Nsteps=5, energy=3.5e9)]),
+        ("WigglerHV", [Wiggler(0.25, lw=0.05, Bmax=0.8, Nsteps=4, By=(1, 1, 1, 1, 1, 0, 2, -1, 0, 3, 3, 1),
+                               Bx=(1, 1, 1, 2, 2, 0), energy=3.5e9)]),
+        ("WigglerRad", [Wiggler(0.3, lw=0.1, Bmax=1.5, Nsteps=3, energy=3.5e9, rad=1)]),
         ("LongitudinalWakeUnsorted", [LongitudinalWake([0.0, 5e-12, 2e-12, 1e-11], [1e13, 2e12, 6e12, -1e12],
                                                        fliphalf=-4.0, scale=2e-19)]),
     ]

@@ -337,8 +337,9 @@ def test_batched_time_dependent_equals_lattice_by_lattice():
 
 def test_array_field_kinds_bitwise():
     """LBend (both signs of the gradient), StrongGaussianBeam slices, the
-    resonator wake and sorted / unsorted tabulated wakes, over a beam whose z
-    spans the wake tables, against the oracle bit for bit."""
+    resonator wake, sorted / unsorted tabulated wakes and wigglers (vertical
+    harmonics, radiation), over a beam whose z spans the wake tables, against
+    the oracle bit for bit."""
     lat = tp.Lattice([
         tp.LBend(0.9, 0.15, 0.03, 0.02, K=0.8, by_error=1e-4, fint1=0.5, fint2=0.4, full_gap=0.05),
         tp.Drift(0.5),
@@ -350,6 +351,9 @@ def test_array_field_kinds_bitwise():
                             fliphalf=-1.0, scale=1e-19),
         tp.LongitudinalWake([0.0, 5e-12, 2e-12, 1e-11], [1e13, 2e12, 6e12, -1e12], fliphalf=-1.0, scale=2e-19),
         tp.Quadrupole(0.4, 1.1),
+        tp.Wiggler(0.2, lw=0.05, Bmax=0.9, Nsteps=3, By=(1, 1, 1, 1, 1, 0, 2, -1, 0, 3, 3, 1),
+                   Bx=(1, 1, 1, 2, 2, 0), energy=3.5e9),
+        tp.Wiggler(0.2, lw=0.1, Bmax=1.4, Nsteps=2, energy=3.5e9, rad=1),
     ])
     beam = tp.Beam(3.5e9)
     c = W.gaussian(4096, seed=77, sigma=(1e-4, 1e-5, 1e-4, 1e-5, 3e-3, 1e-4))

@@ -10,7 +10,7 @@ from .elements import (AbstractElement, AccelCavity, Corrector, CrabCavity, Drif
                        Octupole, OctupoleSC, Quadrupole, QuadrupoleSC, RBend, RBendSC, RFCavity, SBend, SBendSC,
                        Sextupole, SextupoleSC, Solenoid, SpaceCharge, StrongThinGaussianBeam, ThinMultipole,
                        Translation, VKicker, YRotation, LBend, StrongGaussianBeam, LongitudinalRLCWake,
-                       LongitudinalWake)
+                       LongitudinalWake, Wiggler)
 from .tracking import (Batch, Beam, Lattice, Time, TimeContext, TimeDependentParam, TimeVaryingElement, Turn,
                        adjoint_stats, beti, context, last_stats, linepass_, materialize, one_turn_jacobian,
                        probe_fp64_peak, ringpass_, ringpass_adjoint, spos, timed)

@@ -440,6 +440,69 @@ static Rec compile_rec(const tp_elem& e, const AuxView& aux) {
             r.tail.assign(t, t + 2 * n);
             break;
         }
+        case TP_WIGGLER: {  // tracking.jl:1224-1529
+            const double* a = aux.p + e.iparam[0];
+            const int nh = int(a[0]), nv = int(a[1]), rad = int(a[2]);
+            const double lw = e.param[0], bmax = e.param[1], energy = e.param[2];
+            const int PN = e.num_int_steps;
+            const double Nw = std::nearbyint(e.L / lw);  // round(Int, L/lw): half to even
+            const double Nstep = double(PN) * (Nw > 1.0 ? Nw : 1.0);
+            const double dl = lw / double(PN);
+            const double dl1 = dl * 1.3512071919596573, dl0 = dl * -1.7024143839193146;
+            const double Aw = 1e-9 * 2.99792458e8 / (0.51099895069e6 * 1e-9) / TWO_PI * lw * bmax;
+            const double kw = TWO_PI / lw;
+            double Po, srCoef = 0.0;
+            if (rad == 1) {
+                const double gamma = energy / 0.51099895069e6;
+                Po = std::sqrt(gamma * gamma - 1.0);
+                srCoef = (2.0 / 3.0) * 2.8179403205e-15 * (gamma * gamma * gamma);
+            } else {
+                Po = std::sqrt((energy / 0.51099895069e6) * (energy / 0.51099895069e6) - 1.0);
+            }
+            const double H = Po * 0.51099895069e6 / 2.99792458e8;
+            r.h.kind = DK_WIGGLER;
+            r.w[wg::NSTEP] = Nstep;
+            r.w[wg::DL1] = dl1;
+            r.w[wg::DL0] = dl0;
+            r.w[wg::DL1H] = dl1 / 2.0;
+            r.w[wg::DL0H] = dl0 / 2.0;
+            r.w[wg::PO] = Po;
+            r.w[wg::SRCOEF] = srCoef;
+            r.w[wg::SL] = dl;
+            r.w[wg::HH] = H * H;
+            r.w[wg::NH] = double(nh);
+            r.w[wg::NV] = double(nv);
+            r.w[wg::RAD] = double(rad);
+            r.nw = wg::WORDS;
+            r.tail.assign(size_t(wg::HWORDS) * size_t(nh + nv), 0.0);
+            for (int i = 0; i < nh + nv; ++i) {
+                const bool horiz = i < nh;
+                const double* b = a + 3 + 6 * i;
+                double* o = r.tail.data() + size_t(wg::HWORDS) * size_t(i);
+                const double kx = b[2] * kw, ky = b[3] * kw, kz = b[4] * kw;
+                const double c = b[1] * Aw / Po;   // HCw or VCw of the vector potential
+                const double ckz = c * (kw / kz);
+                o[wg::KX] = kx; o[wg::KY] = ky; o[wg::KZ] = kz; o[wg::TZ] = b[5];
+                if (horiz) {
+                    o[wg::C_AX] = ckz;
+                    o[wg::C_AXPY] = ckz * ky;
+                    o[wg::C_AY] = ckz * (kx / ky);
+                    o[wg::C_AYPX] = ckz * ((kx / ky) * (kx / ky));
+                    o[wg::SINC] = std::fabs(kx / kw) > 1e-6 ? 1.0 : 0.0;
+                    o[wg::B_X] = bmax * b[1] * (kx / ky);
+                    o[wg::B_Y] = bmax * b[1];
+                } else {
+                    o[wg::C_AX] = ckz * (ky / kx);
+                    o[wg::C_AXPY] = ckz * ((ky / kx) * (ky / kx));
+                    o[wg::C_AY] = ckz;
+                    o[wg::C_AYPX] = ckz * kx;
+                    o[wg::SINC] = std::fabs(ky / kw) > 1e-6 ? 1.0 : 0.0;
+                    o[wg::B_X] = bmax * b[1];
+                    o[wg::B_Y] = bmax * b[1] * (ky / kx);
+                }
+            }
+            break;
+        }
         default:
             break;
     }
@@ -594,6 +657,34 @@ double elem_flops(const tp_elem& e, const tp_misalign* mis, bool exact, const Au
         case TP_LONGITUDINAL_WAKE:
             // a particle ahead of the wake (z > 0 with fliphalf < 0); one behind adds the interpolation
             return e.param[1] == 0.0 ? 0.0 : 3.0;
+        case TP_WIGGLER: {
+            // per 2nd-order map: 46 operations, 752 per By and 762 per Bx harmonic (each harmonic
+            // costs 5 or 6 transcendental calls per vector-potential evaluation, 6 evaluations per map)
+            // (a By harmonic with kx != 0 evaluates sin(kx x)/kx, 8 operations more than the
+            // small-argument series, in each of the 2 ax evaluations per map; a Bx harmonic with
+            // ky == 0 takes the series, 8 fewer, in each of the 4 ay evaluations per map)
+            const double* a = aux.p + e.iparam[0];
+            const int nh = int(a[0]), nv = int(a[1]);
+            const bool rad = a[2] == 1.0;
+            const double nw = std::nearbyint(e.L / e.param[0]);
+            const double nstep = double(e.num_int_steps) * (nw > 1.0 ? nw : 1.0);
+            double per_step = 138.0, per_block = 24.0;
+            for (int i = 0; i < nh + nv; ++i) {
+                const double* b = a + 3 + 6 * i;
+                if (i < nh) {
+                    const bool sinpath = std::fabs(b[2]) > 1e-6;  // |kx / kw|
+                    per_step += 2256.0 + (sinpath ? 48.0 : 0.0);
+                    per_block += 397.0 + (sinpath ? 8.0 : 0.0);
+                } else {
+                    const bool series = !(std::fabs(b[3]) > 1e-6);  // |ky / kw|
+                    per_step += 2286.0 - (series ? 96.0 : 0.0);
+                    per_block += 405.0 - (series ? 8.0 : 0.0);
+                }
+            }
+            double f = mis_f + 14.0 + nstep * per_step;
+            if (rad) f += 3.0 + (nstep + 1.0) * per_block;
+            return f;
+        }
         default: return 0.0;
     }
 }

@@ -693,6 +693,152 @@ static __device__ __noinline__ void tab_wake(P6& s, const double* w, const RecHd
     s.d = s.d - w[tw::SCALE] * wf;
 }
 
+// Wiggler (src/tracking.jl:1224-1529): 4th-order composition of the
+// second-order map _wig_map_2nd, whose kicks are the vector potential of the
+// By (horizontal) and Bx (vertical) harmonics; optional radiation kicks.
+// Zw, the longitudinal position inside the wiggler, advances by dl/2 twice
+// per map (the same sequence for every particle).
+__device__ __forceinline__ double sinc_taylor(double x) {
+    const double x2 = x * x;
+    return 1.0 - x2 / 6.0 * (1.0 - x2 / 20.0 * (1.0 - x2 / 42.0 * (1.0 - x2 / 72.0)));
+}
+
+static __device__ __noinline__ void wig_ax_axpy(const double* w, double x, double y, double Zw, double& ax, double& axpy) {
+    const int nh = int(w[wg::NH]), nv = int(w[wg::NV]);
+    const double* hp = w + wg::WORDS;
+    ax = 0.0;
+    axpy = 0.0;
+    for (int i = 0; i < nh; ++i, hp += wg::HWORDS) {
+        const double kx = hp[wg::KX], ky = hp[wg::KY];
+        const double cx = libm::cos(kx * x), chy = libm::cosh(ky * y);
+        const double sz = libm::sin(hp[wg::KZ] * Zw + hp[wg::TZ]);
+        ax = ax + hp[wg::C_AX] * cx * chy * sz;
+        const double shy = libm::sinh(ky * y);
+        const double sxkx = hp[wg::SINC] != 0.0 ? libm::sin(kx * x) / kx : x * sinc_taylor(kx * x);
+        axpy = axpy + hp[wg::C_AXPY] * sxkx * shy * sz;
+    }
+    for (int i = 0; i < nv; ++i, hp += wg::HWORDS) {
+        const double kx = hp[wg::KX], ky = hp[wg::KY];
+        const double shx = libm::sinh(kx * x), sy = libm::sin(ky * y);
+        const double sz = libm::sin(hp[wg::KZ] * Zw + hp[wg::TZ]);
+        ax = ax + hp[wg::C_AX] * shx * sy * sz;
+        const double chx = libm::cosh(kx * x), cy = libm::cos(ky * y);
+        axpy = axpy + hp[wg::C_AXPY] * chx * cy * sz;
+    }
+}
+
+static __device__ __noinline__ void wig_ay_aypx(const double* w, double x, double y, double Zw, double& ay, double& aypx) {
+    const int nh = int(w[wg::NH]), nv = int(w[wg::NV]);
+    const double* hp = w + wg::WORDS;
+    ay = 0.0;
+    aypx = 0.0;
+    for (int i = 0; i < nh; ++i, hp += wg::HWORDS) {
+        const double kx = hp[wg::KX], ky = hp[wg::KY];
+        const double sx = libm::sin(kx * x), shy = libm::sinh(ky * y);
+        const double sz = libm::sin(hp[wg::KZ] * Zw + hp[wg::TZ]);
+        ay = ay + hp[wg::C_AY] * sx * shy * sz;
+        const double cx = libm::cos(kx * x), chy = libm::cosh(ky * y);
+        aypx = aypx + hp[wg::C_AYPX] * cx * chy * sz;
+    }
+    for (int i = 0; i < nv; ++i, hp += wg::HWORDS) {
+        const double kx = hp[wg::KX], ky = hp[wg::KY];
+        const double chx = libm::cosh(kx * x), cy = libm::cos(ky * y);
+        const double sz = libm::sin(hp[wg::KZ] * Zw + hp[wg::TZ]);
+        ay = ay + hp[wg::C_AY] * chx * cy * sz;
+        const double shx = libm::sinh(kx * x);
+        const double syky = hp[wg::SINC] != 0.0 ? libm::sin(ky * y) / ky : y * sinc_taylor(ky * y);
+        aypx = aypx + hp[wg::C_AYPX] * shx * syky * sz;
+    }
+}
+
+__device__ __forceinline__ void wig_map_2nd(P6& s, const double* w, double dl, double dl2, double& Zw) {
+    const double inv1pd = 1.0 / (1.0 + s.d);
+    const double dld = dl * inv1pd;
+    const double dl2d = dl2 * inv1pd;
+    Zw = Zw + dl2;
+    double a, ap;
+    wig_ay_aypx(w, s.x, s.y, Zw, a, ap);
+    s.px = s.px - ap;
+    s.py = s.py - a;
+    s.y = s.y + dl2d * s.py;
+    s.z = s.z + (dl2d / 2.0) * (s.py * s.py) * inv1pd;
+    wig_ay_aypx(w, s.x, s.y, Zw, a, ap);
+    s.px = s.px + ap;
+    s.py = s.py + a;
+    wig_ax_axpy(w, s.x, s.y, Zw, a, ap);
+    s.px = s.px - a;
+    s.py = s.py - ap;
+    s.x = s.x + dld * s.px;
+    s.z = s.z + (dld / 2.0) * (s.px * s.px) * inv1pd;
+    wig_ax_axpy(w, s.x, s.y, Zw, a, ap);
+    s.px = s.px + a;
+    s.py = s.py + ap;
+    wig_ay_aypx(w, s.x, s.y, Zw, a, ap);
+    s.px = s.px - ap;
+    s.py = s.py - a;
+    s.y = s.y + dl2d * s.py;
+    s.z = s.z + (dl2d / 2.0) * (s.py * s.py) * inv1pd;
+    wig_ay_aypx(w, s.x, s.y, Zw, a, ap);
+    s.px = s.px + ap;
+    s.py = s.py + a;
+    Zw = Zw + dl2;
+}
+
+// _wig_B (transverse field) and _wig_radiation_kicks, between the removal and
+// the restoration of the vector-potential kick (tracking.jl:1400-1463, 1477-1483).
+static __device__ __noinline__ void wig_rad_block(P6& s, const double* w, double Zw) {
+    double ax, axpy, ay, aypx;
+    wig_ax_axpy(w, s.x, s.y, Zw, ax, axpy);
+    wig_ay_aypx(w, s.x, s.y, Zw, ay, aypx);
+    s.px = s.px - ax;
+    s.py = s.py - ay;
+    const int nh = int(w[wg::NH]), nv = int(w[wg::NV]);
+    const double* hp = w + wg::WORDS;
+    double Bxv = 0.0, Byv = 0.0;
+    for (int i = 0; i < nh; ++i, hp += wg::HWORDS) {
+        const double kx = hp[wg::KX], ky = hp[wg::KY];
+        const double sx = libm::sin(kx * s.x), cx = libm::cos(kx * s.x);
+        const double chy = libm::cosh(ky * s.y), shy = libm::sinh(ky * s.y);
+        const double cz = libm::cos(hp[wg::KZ] * Zw + hp[wg::TZ]);
+        Bxv = Bxv + hp[wg::B_X] * sx * shy * cz;
+        Byv = Byv - hp[wg::B_Y] * cx * chy * cz;
+    }
+    for (int i = 0; i < nv; ++i, hp += wg::HWORDS) {
+        const double kx = hp[wg::KX], ky = hp[wg::KY];
+        const double shx = libm::sinh(kx * s.x), chx = libm::cosh(kx * s.x);
+        const double sy = libm::sin(ky * s.y), cy = libm::cos(ky * s.y);
+        const double cz = libm::cos(hp[wg::KZ] * Zw + hp[wg::TZ]);
+        Bxv = Bxv + hp[wg::B_X] * chx * cy * cz;
+        Byv = Byv - hp[wg::B_Y] * shx * sy * cz;
+    }
+    const double B2 = Bxv * Bxv + Byv * Byv;
+    if (B2 != 0.0) {
+        const double irho2 = B2 / w[wg::HH];
+        const double dFactor = (1.0 + s.d) * (1.0 + s.d);
+        const double dDelta = -w[wg::SRCOEF] * dFactor * irho2 * w[wg::SL];
+        const double scale = 1.0 + dDelta;
+        s.px = s.px * scale;
+        s.py = s.py * scale;
+        s.d = s.d + dDelta;
+    }
+    s.px = s.px + ax;
+    s.py = s.py + ay;
+}
+
+static __device__ __noinline__ void wiggler(P6& s, const double* w) {
+    const long long nstep = (long long)w[wg::NSTEP];
+    const double dl1 = w[wg::DL1], dl0 = w[wg::DL0], dl1h = w[wg::DL1H], dl0h = w[wg::DL0H];
+    const bool rad = w[wg::RAD] == 1.0;
+    double Zw = 0.0;
+    if (rad) wig_rad_block(s, w, Zw);
+    for (long long k = 0; k < nstep; ++k) {
+        wig_map_2nd(s, w, dl1, dl1h, Zw);
+        wig_map_2nd(s, w, dl0, dl0h, Zw);
+        wig_map_2nd(s, w, dl1, dl1h, Zw);
+        if (rad) wig_rad_block(s, w, Zw);
+    }
+}
+
 // Misalignment (src/tracking.jl:60-67): r + t, and the column-major 6x6 product.
 __device__ __forceinline__ void mat6(const double* R, P6& s) {
     double v[6] = {s.x, s.px, s.y, s.py, s.z, s.d};
@@ -785,6 +931,7 @@ __device__ __forceinline__ bool apply_record(P6& s, const double* rec, const Rec
         case DK_SGB: strong_gauss(s, w); break;
         case DK_RLC_WAKE: rlc_wake(s, w); break;
         case DK_TAB_WAKE: tab_wake(s, w, h); break;
+        case DK_WIGGLER: wiggler(s, w); break;
         case DK_NAN: set_nan(s); break;
         default: return false;
     }

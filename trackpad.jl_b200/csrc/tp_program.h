@@ -114,6 +114,14 @@ enum { L = 0, KX = 1, G1C = 2, NGRD = 3, BYERR = 4, IRHO = 5, FX_IN = 6, E_IN = 
 namespace sgb { enum { FACTOR = 0, SX2 = 1, SY2 = 2, NZ = 3, WORDS = 4 }; }  // then w[nz], xo[nz], yo[nz]
 namespace rlc { enum { SCALE = 0, A = 1, W0P = 2, D2Q0P = 3, W0 = 4, D2Q0 = 5, WORDS = 6 }; }
 namespace tw { enum { SCALE = 0, FLIP = 1, T1F = 2, N = 3, WORDS = 4 }; }  // then times[n], wakes[n]
+namespace wg {  // DK_WIGGLER, then HWORDS words per harmonic (By harmonics first, then Bx)
+enum { NSTEP = 0, DL1 = 1, DL0 = 2, DL1H = 3, DL0H = 4, PO = 5, SRCOEF = 6, SL = 7, HH = 8, NH = 9, NV = 10,
+       RAD = 11, WORDS = 12 };
+// per harmonic: wave numbers, phase, the four vector-potential coefficients,
+// the small-argument flag of sin(k u)/k, and the two field coefficients
+enum { KX = 0, KY = 1, KZ = 2, TZ = 3, C_AX = 4, C_AXPY = 5, C_AY = 6, C_AYPX = 7, SINC = 8, B_X = 9,
+       B_Y = 10, HWORDS = 12 };
+}
 
 // Misalignment row as stored on the device (same content as tp_misalign).
 struct MisalignDev {

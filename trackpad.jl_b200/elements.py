@@ -540,7 +540,31 @@ class LongitudinalWake(AbstractElement):
         return 0.0
 
 
+class Wiggler(AbstractElement):
+    """src/elements/wiggler.jl:6-44: harmonics By / Bx of six integers each
+    (_, amplitude, kx/kw, ky/kw, kz/kw, phase)."""
+    kind = "WIGGLER"
+    _misalignable = True
+
+    def __init__(self, L, *, name="WIGGLER", lw=0.0, Bmax=0.0, Nsteps=10, By=(1, 1, 0, 1, 1, 0), Bx=(),
+                 energy=1.0e9, rad=0, t1=None, t2=None, r1=None, r2=None):
+        self.name = name
+        self.L, self.lw, self.Bmax, self.Nsteps = float(L), float(lw), float(Bmax), int(Nsteps)
+        self.By = [int(v) for v in By]
+        self.Bx = [int(v) for v in Bx]
+        self.NHharm, self.NVharm = len(self.By) // 6, len(self.Bx) // 6
+        self.energy, self.rad = float(energy), int(rad)
+        self._misalign_init(t1, t2, r1, r2)
+
+    def _fields(self):
+        by = [float(v) for v in self.By[:6 * self.NHharm]]
+        bx = [float(v) for v in self.Bx[:6 * self.NVharm]]
+        return {"L": self.L, "num_int_steps": self.Nsteps, "param": [self.lw, self.Bmax, self.energy] + [0.0] * 5,
+                "aux": [float(self.NHharm), float(self.NVharm), float(self.rad)] + by + bx}
+
+
 ELEMENT_TYPES = [Marker, Drift, Quadrupole, Sextupole, Octupole, ThinMultipole, SBend, ExactSBend, RFCavity,
                  Solenoid, Corrector, Translation, YRotation, CrabCavity, AccelCavity, LongitudinalRFMap,
                  LorentzBoost, InvLorentzBoost, SpaceCharge, DriftSC, QuadrupoleSC, SextupoleSC, OctupoleSC,
-                 SBendSC, StrongThinGaussianBeam, LBend, StrongGaussianBeam, LongitudinalRLCWake, LongitudinalWake]
+                 SBendSC, StrongThinGaussianBeam, LBend, StrongGaussianBeam, LongitudinalRLCWake, LongitudinalWake,
+                 Wiggler]

@@ -50,7 +50,8 @@ const TP_KIND = Dict{DataType,Int32}(
     SBend => 6, ExactSBend => 7, RFCavity => 8, Solenoid => 9, Corrector => 10, Translation => 11,
     YRotation => 12, CrabCavity => 13, AccelCavity => 14, LongitudinalRFMap => 15, LorentzBoost => 16,
     InvLorentzBoost => 17, SpaceCharge => 18, DriftSC => 19, QuadrupoleSC => 20, SextupoleSC => 21,
-    OctupoleSC => 22, SBendSC => 23, StrongThinGaussianBeam => 24)
+    OctupoleSC => 22, SBendSC => 23, StrongThinGaussianBeam => 24, LBend => 25, Wiggler => 26,
+    StrongGaussianBeam => 27, LongitudinalRLCWake => 28, LongitudinalWake => 29)
 
 check(st, what) = st == 0 || error("$what: " * unsafe_string(ccall((:tp_strerror, LIB), Cstring, (Cint,), st)) *
                                    " (" * unsafe_string(ccall((:tp_last_error_string, LIB), Cstring, ())) * ")")
@@ -63,13 +64,32 @@ _rf_k(rf) = hasproperty(rf, :k) ? Float64(rf.k) : 0.0
 _rf_h(rf::CrabCavity) = 1.0
 _rf_h(rf) = hasproperty(rf, :h) ? Float64(rf.h) : 1.0
 
+"""The array fields of an element, appended to `aux` (include/trackpad_b200.h
+lists the layout per kind); returns (offset, length) for iparam."""
+function pack_arrays!(aux::Vector{Float64}, e)
+    off = length(aux)
+    if e isa StrongGaussianBeam
+        n = max(e.nzslice, 0)
+        append!(aux, [i <= length(e.zslice_npar) ? e.zslice_npar[i] : 1.0 / n for i in 1:n])
+        append!(aux, [i <= length(e.xoffsets) ? e.xoffsets[i] : 0.0 for i in 1:n])
+        append!(aux, [i <= length(e.yoffsets) ? e.yoffsets[i] : 0.0 for i in 1:n])
+    elseif e isa LongitudinalWake
+        append!(aux, Float64.(e.times)); append!(aux, Float64.(e.wakefields))
+    elseif e isa Wiggler
+        append!(aux, Float64[e.NHharm, e.NVharm, e.rad])
+        append!(aux, Float64.(e.By[1:6e.NHharm])); append!(aux, Float64.(e.Bx[1:6e.NVharm]))
+    end
+    (Int32(off), Int32(length(aux) - off))
+end
+
 """Pack one TrackPad element into the C record (fields by reference name)."""
-function pack(e::AbstractElement, mis_index::Int32)
+function pack(e::AbstractElement, mis_index::Int32, aux::Vector{Float64} = Float64[])
     T = typeof(e).name.wrapper
     kind = get(TP_KIND, T, Int32(-1))
     kind < 0 && throw(ArgumentError("element $(T) has no device implementation"))
     k = e isa Quadrupole ? e.k1 : e isa Sextupole ? e.k2 : e isa Octupole ? e.k3 : 0.0
     p = zeros(8); ip = (Int32(0), Int32(0))
+    gap = field(e, :gap, 0.0)
     if e isa Solenoid; p[1] = e.ks
     elseif e isa Corrector; p[1] = e.xkick; p[2] = e.ykick
     elseif e isa Translation; p[1:3] .= (e.dx, e.dy, e.ds)
@@ -80,13 +100,19 @@ function pack(e::AbstractElement, mis_index::Int32)
     elseif e isa InvLorentzBoost; p[1:4] .= (e.angle, e.cosang, e.sinang, 0.0); ip = (Int32(e.mode), Int32(0))
     elseif e isa Union{QuadrupoleSC,SextupoleSC,OctupoleSC}; p[1:4] .= (e.k0, e.k1, e.k2, e.k3)
     elseif e isa StrongThinGaussianBeam; p[1:5] .= (e.amplitude, e.rmssizex, e.rmssizey, e.xoffset, e.yoffset)
+    elseif e isa LBend; p[1:2] .= (e.K, e.by_error); gap = e.full_gap
+    elseif e isa LongitudinalRLCWake; p[1:4] .= (e.freq, e.Rshunt, e.Q0, e.scale)
+    elseif e isa StrongGaussianBeam; p[1:4] .= (e.charge, e.total_energy, e.beamsize[1], e.beamsize[2])
+        ip = pack_arrays!(aux, e)
+    elseif e isa LongitudinalWake; p[1:2] .= (e.fliphalf, e.scale); ip = pack_arrays!(aux, e)
+    elseif e isa Wiggler; p[1:3] .= (e.lw, e.Bmax, e.energy); ip = pack_arrays!(aux, e)
     end
     TpElem(kind, Int32(hasproperty(e, :max_order) ? e.max_order : 0),
-           Int32(hasproperty(e, :num_int_steps) ? e.num_int_steps : 0),
+           Int32(hasproperty(e, :num_int_steps) ? e.num_int_steps : (e isa Wiggler ? e.Nsteps : 0)),
            Int32(hasproperty(e, :fringe_bend_entrance) ? e.fringe_bend_entrance : 0),
            Int32(hasproperty(e, :fringe_bend_exit) ? e.fringe_bend_exit : 0), mis_index, ip,
            field(e, :L, 0.0), Float64(k), field(e, :angle, 0.0), field(e, :e1, 0.0), field(e, :e2, 0.0),
-           field(e, :fint1, 0.0), field(e, :fint2, 0.0), field(e, :gap, 0.0), field(e, :gk, 0.0),
+           field(e, :fint1, 0.0), field(e, :fint2, 0.0), gap, field(e, :gk, 0.0),
            vec4(e, :polynom_a), vec4(e, :polynom_b),
            hasproperty(e, :kick_angle) ? NTuple{2,Float64}(e.kick_angle) : (0.0, 0.0),
            field(e, :volt, 0.0), field(e, :freq, 0.0), field(e, :h, 0.0), field(e, :lag, 0.0),
@@ -101,7 +127,7 @@ mutable struct DeviceLattice
 end
 
 function DeviceLattice(lat::Lattice; strengths = nothing)
-    elems = TpElem[]; mis = TpMisalign[]
+    elems = TpElem[]; mis = TpMisalign[]; aux = Float64[]
     for e in lat.elements
         b = e isa TimeVaryingElement ? e.base : e
         idx = Int32(-1)
@@ -109,7 +135,7 @@ function DeviceLattice(lat::Lattice; strengths = nothing)
             push!(mis, TpMisalign(Tuple(b.t1), Tuple(b.t2), Tuple(vec(b.r1)), Tuple(vec(b.r2))))
             idx = Int32(length(mis) - 1)
         end
-        push!(elems, pack(b, idx))
+        push!(elems, pack(b, idx, aux))
     end
     if strengths !== nothing  # (element indices, values): the main strength k of those records
         for (i, k) in zip(strengths...)
@@ -119,9 +145,11 @@ function DeviceLattice(lat::Lattice; strengths = nothing)
         end
     end
     h = Ref{Ptr{Cvoid}}(C_NULL)
-    GC.@preserve elems mis begin
-        check(ccall((:tp_lattice_create, LIB), Cint, (Ptr{TpElem}, Int64, Ptr{TpMisalign}, Int64, Ref{Ptr{Cvoid}}),
-                    elems, length(elems), isempty(mis) ? C_NULL : mis, length(mis), h), "tp_lattice_create")
+    GC.@preserve elems mis aux begin
+        check(ccall((:tp_lattice_create_ex, LIB), Cint,
+                    (Ptr{TpElem}, Int64, Ptr{TpMisalign}, Int64, Ptr{Float64}, Int64, Ref{Ptr{Cvoid}}),
+                    elems, length(elems), isempty(mis) ? C_NULL : mis, length(mis),
+                    isempty(aux) ? C_NULL : aux, length(aux), h), "tp_lattice_create_ex")
     end
     d = DeviceLattice(h[])
     finalizer(x -> ccall((:tp_lattice_destroy, LIB), Cint, (Ptr{Cvoid},), x.handle), d)
