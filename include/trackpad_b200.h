@@ -336,7 +336,10 @@ TP_API int tp_ringpass_batched(tp_ctx* ctx, tp_batch* b,
  *   loss = mean_s (x_s^2 + y_s^2) / sigma^2 + lost_weight * (lost / alive-at-start)
  * The gradient is taken with respect to the main strength `k` of the listed
  * elements (Quadrupole k1, Sextupole k2, Octupole k3); the survivor set is
- * held fixed, so the piecewise-constant loss term contributes nothing. */
+ * held fixed, so the piecewise-constant loss term contributes nothing.
+ * Every element kind and every misalignment row can be differentiated; a
+ * misalignment row whose r1 or r2 is singular (no inverse map) gives
+ * TP_EUNSUPPORTED, here and in tp_one_turn_jacobian. */
 enum tp_loss_kind { TP_LOSS_BEAM_SIZE = 0 };
 typedef struct tp_loss_spec {
     int32_t kind;

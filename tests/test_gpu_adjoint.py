@@ -291,7 +291,3 @@ def test_adjoint_rejects_what_it_cannot_differentiate():
         tp.ringpass_adjoint(c0, lat, beam, None, 2, [drift], sigma=SIGMA)
     with pytest.raises(ValueError):
         tp.ringpass_adjoint(c0, lat, beam, None, 2, [10 ** 6], sigma=SIGMA)
-    sol = tp.Lattice(list(lat.elements) + [tp.Solenoid(0.5, 0.3)])
-    with pytest.raises(tp._abi.TrackPadError) as ei:
-        tp.ringpass_adjoint(c0, sol, beam, None, 2, [], sigma=SIGMA)
-    assert ei.value.status == tp._abi.TP_EUNSUPPORTED

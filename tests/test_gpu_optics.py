@@ -64,3 +64,16 @@ def test_batched_maps_at_many_momenta():
     R = oracle_ref.jacobian(lat, refs, tp.beti(beam))
     assert np.abs(M - R).max() <= 1e-9 * np.abs(R).max()
     assert (err < 1e-10).all()
+
+
+def test_finite_difference_map_is_the_references_bit_for_bit():
+    """method="fd" tracks the reference's 12 orbits on the device; the tracking
+    is bit-identical to the oracle's, so the matrix is too."""
+    lat, beam = W.dba_ring(cells=3), W.dba_beam()
+    ref = np.array([2e-5, -1e-6, 1e-5, 0.0, 1e-4, 5e-4])
+    M = tp.optics.one_turn_map(lat, beam, ref, method="fd")
+    c = tp.optics.fd_orbits(ref)
+    oracle_ref.ringpass(lat, c, np.zeros(12, np.int64), tp.beti(beam), 1, aperture=(1.0, 1.0))
+    assert np.array_equal(M, tp.optics.fd_assemble(c))
+    E = tp.optics.one_turn_map(lat, beam, ref)
+    assert np.abs(M - E).max() < 1e-6 * np.abs(E).max()

@@ -91,3 +91,20 @@ def test_tune_from_a_known_2x2_map():
         assert abs(q - (mu / (2 * math.pi)) % 1.0) < 1e-14
     with pytest.raises(ValueError):
         tp.optics.twiss_from_2x2(np.array([[2.0, 1.0], [1.0, 1.0]]))
+
+
+def test_fd_map_assembly_against_the_oracle():
+    """fd_orbits/fd_assemble (the reference's one_turn_map, src/optics.jl:110-121)
+    with the oracle as the tracker agree with the oracle's dual-number map to
+    the truncation error of h = 1e-8 central differences."""
+    import oracle_ref
+    W = __import__("trackpad_b200.workloads", fromlist=["x"])
+    lat, beam = W.dba_ring(cells=2), W.dba_beam()
+    ref = np.array([1e-5, 0.0, -2e-5, 0.0, 0.0, 1e-4])
+    c = tp.optics.fd_orbits(ref)
+    assert c.flags.f_contiguous and c.shape == (12, 6)
+    assert np.array_equal(c[4], ref + 1e-8 * np.eye(6)[2]) and np.array_equal(c[5], ref - 1e-8 * np.eye(6)[2])
+    oracle_ref.ringpass(lat, c, np.zeros(12, np.int64), tp.beti(beam), 1)
+    M = tp.optics.fd_assemble(c)
+    R = oracle_ref.jacobian(lat, ref[None, :], tp.beti(beam))[0]
+    assert np.abs(M - R).max() < 1e-6 * np.abs(R).max()

@@ -6,6 +6,7 @@ reference operation for operation).  Host code is compiled without FMA
 contraction so that hoisted element constants are bit-identical to the values
 the reference computes per particle.
 """
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -48,20 +49,22 @@ def build(verbose=False, ptxas_info=False):
         ("tp_noalloc.o", "tp_noalloc.cu", ["-fmad=false"]),
     ]
     objs = []
-    log = []
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
     deps.append(os.path.join(HERE, "..", "include", "trackpad_b200.h"))
     newest_dep = max(os.path.getmtime(d) for d in deps)
-    relinked = False
+    jobs = []
     for obj, src, extra in units:
         o = os.path.join(BUILD, obj)
         s = os.path.join(CSRC, src)
         stale = (not os.path.exists(o) or os.path.getmtime(o) < max(os.path.getmtime(s), newest_dep)
                  or os.environ.get("TP_REBUILD") or ptxas_info)
         if stale:
-            log.append(_run(base + extra + ["-c", s, "-o", o]))
-            relinked = True
+            jobs.append(base + extra + ["-c", s, "-o", o])
         objs.append(o)
+    # the translation units are independent: compile them concurrently
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        log = list(ex.map(_run, jobs))
+    relinked = bool(jobs)
     if relinked or not os.path.exists(OUT) or os.path.getmtime(OUT) < max(os.path.getmtime(o) for o in objs):
         _run([nvcc(), *ARCH, "-shared", "-o", OUT, *objs, "-Xcompiler", "-fPIC", "-cudart", "static"])
     if verbose:

@@ -11,7 +11,8 @@
 //           K-th turn (the checkpoints) and at the end;
 //  reverse  walks each K-turn segment backwards from the stored state at its
 //           end, rebuilding the state before every building block with the
-//           block's exact time-reversed map (tp_reverse.cuh) while pulling
+//           block's exact time-reversed map (tp_reverse.cuh,
+//           tp_reverse_kinds.cuh) while pulling
 //           the cotangent back through it.  At the start of the segment the
 //           rebuilt state is compared with the stored one (the reconstruction
 //           error reported in tp_adjoint_stats).
@@ -38,7 +39,7 @@
 
 #include "tp_internal.h"
 #include "tp_maps.cuh"
-#include "tp_reverse.cuh"
+#include "tp_reverse_kinds.cuh"
 
 namespace tp {
 namespace {
@@ -66,6 +67,8 @@ struct AdjArgs {
     const int32_t* einfo;     // per element: record word offset, parameter code (slot*4 + pm, or -1)
     const double* sched;
     const AdjVar* var;
+    const MisalignDev* mis;   // misalignment rows of every variant (record aux indexes them)
+    const double* misinv;     // their inverses, 72 words per row (r1^-1, r2^-1)
     int32_t nvar;
     int32_t nturns;
     int32_t turn0;
@@ -128,7 +131,7 @@ __device__ void stage_plain(double* dst, const double* tab, int words_tab, const
     __syncthreads();
 }
 
-template <bool EXACT>
+template <bool EXACT, bool RARE>
 __global__ void __launch_bounds__(kAdjBlock, 4) adj_forward(AdjArgs a) {
     extern __shared__ __align__(16) double smem[];
     const int lane = threadIdx.x & 31;
@@ -167,7 +170,7 @@ __global__ void __launch_bounds__(kAdjBlock, 4) adj_forward(AdjArgs a) {
                 RecHdr h = h0;
                 const double* r = resolve_rec(rec, h, a.sched, V, a.turn0 + t);
                 P6 sn = s;
-                if (r == nullptr || !apply_record<EXACT>(sn, r, h, nullptr, beti, beta, beta2)) {
+                if (r == nullptr || !apply_record<EXACT, RARE>(sn, r, h, RARE ? a.mis : nullptr, beti, beta, beta2)) {
                     atomicOr(a.err, r == nullptr ? DE_SCHED_RANGE : DE_BAD_KIND);
                     act = false;
                     lf = 1;
@@ -196,7 +199,7 @@ __global__ void __launch_bounds__(kAdjBlock, 4) adj_forward(AdjArgs a) {
     }
 }
 
-template <bool EXACT>
+template <bool EXACT, bool RARE>
 __global__ void __launch_bounds__(kAdjBlock, 4) adj_reverse(AdjArgs a) {
     extern __shared__ __align__(16) double smem[];
     const int lane = threadIdx.x & 31;
@@ -253,7 +256,7 @@ __global__ void __launch_bounds__(kAdjBlock, 4) adj_reverse(AdjArgs a) {
                     RecHdr h = *reinterpret_cast<const RecHdr*>(rec);
                     const double* r = resolve_rec(rec, h, a.sched, V, a.turn0 + t);
                     const int pm = code >= 0 ? (code & 3) : 0;
-                    if (r == nullptr || !reverse_record<EXACT>(s, l, r, h, beti, beta2, pm, g))
+                    if (r == nullptr || !reverse_record<EXACT, RARE>(s, l, r, h, a.mis, a.misinv, beti, beta, beta2, pm, g))
                         atomicOr(a.err, r == nullptr ? DE_SCHED_RANGE : DE_BAD_KIND);
                 }
                 if (code >= 0) {  // warp-uniform: every lane walks the same variant
@@ -387,15 +390,19 @@ int cuda_fail(cudaError_t e, const char* where) {
     } while (0)
 
 // Scratch slots of the context used here.
-enum Slot { S_TABLE = 0, S_INFO, S_SCHED, S_VAR, S_COORDS0, S_LOST0, S_FIN, S_LOST, S_CKPT, S_PARTIAL, S_TILES, S_OUT };
+enum Slot { S_TABLE = 0, S_INFO, S_SCHED, S_VAR, S_COORDS0, S_LOST0, S_FIN, S_LOST, S_CKPT, S_PARTIAL, S_TILES, S_OUT,
+            S_MIS };
 
 struct HostPlan {
     std::vector<double> table;
     std::vector<int32_t> einfo;
     std::vector<double> sched;
     std::vector<AdjVar> var;
+    std::vector<MisalignDev> mis;
+    std::vector<double> misinv;
     std::vector<int32_t> param_off;
     int64_t ntot = 0, ntiles = 0, prow_words = 0;
+    bool rare = false;  // kinds outside the integrator core or misalignment rows: the full kernels
 };
 
 double adjoint_stats_time(std::chrono::steady_clock::time_point t0) {
@@ -404,6 +411,53 @@ double adjoint_stats_time(std::chrono::steady_clock::time_point t0) {
 
 thread_local tp_adjoint_stats g_adj_stats{};
 thread_local int64_t g_last_alive = 0;  // particles alive at the start of the last call
+
+// Inverse of a column-major 6x6 matrix by Gauss-Jordan elimination with
+// partial pivoting in long double.  Returns false for a singular matrix.
+bool invert6(const double* R, double* out) {
+    long double a[6][12];
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) {
+            a[i][j] = R[j * 6 + i];
+            a[i][6 + j] = i == j ? 1.0L : 0.0L;
+        }
+    long double scale = 0.0L;
+    for (int k = 0; k < 36; ++k) scale = std::max(scale, std::fabs((long double)R[k]));
+    if (!(scale > 0.0L)) return false;
+    for (int c = 0; c < 6; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < 6; ++r)
+            if (std::fabs(a[r][c]) > std::fabs(a[piv][c])) piv = r;
+        if (!(std::fabs(a[piv][c]) > 1e-14L * scale)) return false;
+        if (piv != c)
+            for (int j = 0; j < 12; ++j) std::swap(a[c][j], a[piv][j]);
+        const long double p = a[c][c];
+        for (int j = 0; j < 12; ++j) a[c][j] /= p;
+        for (int r = 0; r < 6; ++r) {
+            if (r == c || a[r][c] == 0.0L) continue;
+            const long double f = a[r][c];
+            for (int j = 0; j < 12; ++j) a[r][j] -= f * a[c][j];
+        }
+    }
+    for (int i = 0; i < 6; ++i)
+        for (int j = 0; j < 6; ++j) out[j * 6 + i] = double(a[i][6 + j]);
+    return true;
+}
+
+// Shift the misalignment row index of every misaligned record in `words`
+// words of records (the rows of several variants are concatenated).
+void rebase_misalign(double* recs, size_t words, int32_t mbase) {
+    for (size_t w = 0; w < words;) {
+        RecHdr h;
+        std::memcpy(&h, recs + w, sizeof h);
+        if (h.words == 0) break;  // padding word
+        if (h.flags & RF_MISALIGN) {
+            h.aux += mbase;
+            std::memcpy(recs + w, &h, sizeof h);
+        }
+        w += h.words;
+    }
+}
 
 // Build the concatenated device description of `lats`.  params: element
 // indices per variant (param_off[v]..param_off[v+1]), or none (Jacobian).
@@ -417,7 +471,20 @@ int make_plan(const std::vector<const tp_lattice*>& lats, const std::vector<int6
     for (int v = 0; v < nvar; ++v) {
         LatticeHost L;
         lattice_host(lats[size_t(v)], &L);
-        if (L.nmis > 0) return fail(TP_EUNSUPPORTED, "the adjoint does not take misaligned lattices");
+        const int32_t mbase = int32_t(P->mis.size());
+        for (int64_t k = 0; k < L.nmis; ++k) {
+            const tp_misalign& m = L.mis[k];
+            MisalignDev o{};
+            std::memcpy(o.t1, m.t1, sizeof o.t1); std::memcpy(o.t2, m.t2, sizeof o.t2);
+            std::memcpy(o.r1, m.r1, sizeof o.r1); std::memcpy(o.r2, m.r2, sizeof o.r2);
+            for (int q = 0; q < 36; ++q) { o.r1nz |= m.r1[q] != 0.0; o.r2nz |= m.r2[q] != 0.0; }
+            double inv[72] = {};
+            if ((o.r1nz && !invert6(m.r1, inv)) || (o.r2nz && !invert6(m.r2, inv + 36)))
+                return fail(TP_EUNSUPPORTED, "misalignment row " + std::to_string(k) +
+                                                 " has a singular rotation matrix (no inverse map)");
+            P->mis.push_back(o);
+            P->misinv.insert(P->misinv.end(), inv, inv + 72);
+        }
         if (L.has_schedule && (int64_t(turn0) < L.sched_turn0 ||
                                int64_t(turn0) + nturns > int64_t(L.sched_turn0) + L.sched_nturns))
             return fail(TP_ERANGE, "turns outside the lattice schedule");
@@ -442,9 +509,11 @@ int make_plan(const std::vector<const tp_lattice*>& lats, const std::vector<int6
         }
         if (L.has_schedule && !check(L.sched, L.sched_words))
             return fail(TP_EUNSUPPORTED, "a scheduled element has no reverse map yet");
+        if (L.nmis > 0 || records_have_rare(L.program, L.words)) P->rare = true;
         AdjVar& V = P->var[size_t(v)];
         V.toff = int64_t(P->table.size());
         P->table.insert(P->table.end(), L.program, L.program + L.words);
+        if (mbase > 0) rebase_misalign(P->table.data() + V.toff, L.words, mbase);
         while (P->table.size() % 2) P->table.push_back(0.0);
         V.eoff = eoff;
         std::vector<int32_t> code(size_t(L.nelem), -1);
@@ -469,6 +538,7 @@ int make_plan(const std::vector<const tp_lattice*>& lats, const std::vector<int6
         if (L.has_schedule) {
             V.soff = int64_t(P->sched.size());
             P->sched.insert(P->sched.end(), L.sched, L.sched + L.sched_words);
+            if (mbase > 0) rebase_misalign(P->sched.data() + V.soff, L.sched_words, mbase);
         }
         V.sstride = L.sched_stride;
         V.sturn0 = L.sched_turn0;
@@ -539,6 +609,14 @@ int run_adjoint(tp_ctx* c, const std::vector<const tp_lattice*>& lats, const std
         (st = ctx_scratch(c, S_TILES, size_t(P.ntiles) * 32 + 64, &d_tiles)) ||
         (st = ctx_scratch(c, S_OUT, (size_t(nvar) * 2 + size_t(P.param_off.back()) + 8) * 8, &d_out)))
         return st;
+    void* d_mis = nullptr;
+    const size_t mis_bytes = P.mis.size() * sizeof(MisalignDev);
+    if (!P.mis.empty()) {
+        if ((st = ctx_scratch(c, S_MIS, mis_bytes + P.misinv.size() * 8, &d_mis))) return st;
+        ADJ_CUDA(cudaMemcpyAsync(d_mis, P.mis.data(), mis_bytes, cudaMemcpyHostToDevice, s));
+        ADJ_CUDA(cudaMemcpyAsync(static_cast<char*>(d_mis) + mis_bytes, P.misinv.data(), P.misinv.size() * 8,
+                                 cudaMemcpyHostToDevice, s));
+    }
     ADJ_CUDA(cudaMemcpyAsync(d_table, P.table.data(), P.table.size() * 8, cudaMemcpyHostToDevice, s));
     ADJ_CUDA(cudaMemcpyAsync(d_info, P.einfo.data(), P.einfo.size() * 4, cudaMemcpyHostToDevice, s));
     if (!P.sched.empty())
@@ -555,6 +633,8 @@ int run_adjoint(tp_ctx* c, const std::vector<const tp_lattice*>& lats, const std
     a.einfo = static_cast<const int32_t*>(d_info);
     a.sched = static_cast<const double*>(d_sched);
     a.var = static_cast<const AdjVar*>(d_var);
+    a.mis = static_cast<const MisalignDev*>(d_mis);
+    a.misinv = d_mis ? reinterpret_cast<const double*>(static_cast<char*>(d_mis) + mis_bytes) : nullptr;
     a.nvar = nvar;
     a.nturns = nturns;
     a.turn0 = turn0;
@@ -592,23 +672,31 @@ int run_adjoint(tp_ctx* c, const std::vector<const tp_lattice*>& lats, const std
     ADJ_CUDA(cudaEventCreate(&e1));
     ADJ_CUDA(cudaEventCreate(&e2));
     auto cleanup = [&]() { cudaEventDestroy(e0); cudaEventDestroy(e1); cudaEventDestroy(e2); };
+    const bool rare = P.rare;
+    auto set_smem = [&](auto fwd, auto rev) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        return e == cudaSuccess ? cudaFuncSetAttribute(rev, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)) : e;
+    };
     if (smem > 48 * 1024) {
-        cudaError_t e = exact ? cudaFuncSetAttribute(adj_forward<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))
-                              : cudaFuncSetAttribute(adj_forward<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e == cudaSuccess)
-            e = exact ? cudaFuncSetAttribute(adj_reverse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem))
-                      : cudaFuncSetAttribute(adj_reverse<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaError_t e = exact ? (rare ? set_smem(adj_forward<true, true>, adj_reverse<true, true>)
+                                      : set_smem(adj_forward<true, false>, adj_reverse<true, false>))
+                              : (rare ? set_smem(adj_forward<false, true>, adj_reverse<false, true>)
+                                      : set_smem(adj_forward<false, false>, adj_reverse<false, false>));
         if (e != cudaSuccess) { cleanup(); return cuda_fail(e, "cudaFuncSetAttribute"); }
     }
     cudaEventRecord(e0, s);
     if (grid > 0) {
-        if (exact) adj_forward<true><<<grid, kAdjBlock, smem, s>>>(a);
-        else adj_forward<false><<<grid, kAdjBlock, smem, s>>>(a);
+        if (exact && rare) adj_forward<true, true><<<grid, kAdjBlock, smem, s>>>(a);
+        else if (exact) adj_forward<true, false><<<grid, kAdjBlock, smem, s>>>(a);
+        else if (rare) adj_forward<false, true><<<grid, kAdjBlock, smem, s>>>(a);
+        else adj_forward<false, false><<<grid, kAdjBlock, smem, s>>>(a);
     }
     cudaEventRecord(e1, s);
     if (grid > 0) {
-        if (exact) adj_reverse<true><<<grid, kAdjBlock, smem, s>>>(a);
-        else adj_reverse<false><<<grid, kAdjBlock, smem, s>>>(a);
+        if (exact && rare) adj_reverse<true, true><<<grid, kAdjBlock, smem, s>>>(a);
+        else if (exact) adj_reverse<true, false><<<grid, kAdjBlock, smem, s>>>(a);
+        else if (rare) adj_reverse<false, true><<<grid, kAdjBlock, smem, s>>>(a);
+        else adj_reverse<false, false><<<grid, kAdjBlock, smem, s>>>(a);
     }
     cudaEventRecord(e2, s);
     cudaError_t le = cudaGetLastError();

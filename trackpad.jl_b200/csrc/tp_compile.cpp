@@ -689,4 +689,15 @@ double elem_flops(const tp_elem& e, const tp_misalign* mis, bool exact, const Au
     }
 }
 
+bool records_have_rare(const double* recs, size_t words) {
+    for (size_t w = 0; w < words;) {
+        RecHdr h;
+        std::memcpy(&h, recs + w, sizeof h);
+        if (h.words == 0) break;  // padding word
+        if (h.kind > DK_RF) return true;
+        w += h.words;
+    }
+    return false;
+}
+
 }  // namespace tp

@@ -33,7 +33,7 @@ struct TrackArgs {
     int32_t sched_stride;       // words per turn block
     int32_t sched_turn0;
     int32_t sched_nturns;
-    int32_t pad0;
+    int32_t rare;               // the table holds kinds outside the integrator core (kind > DK_RF)
     const MisalignDev* mis;
     double* coords;             // N x 6 column-major
     int64_t n;
@@ -68,6 +68,11 @@ enum DevErr : int32_t {
     DE_TMA_TIMEOUT = 4,
 };
 
+// True when a record of `words` words of records (a compiled table) has a
+// kind outside the integrator core; the tracking kernels without the rare
+// kinds' dispatch run every other table (tp_compile.cpp).
+bool records_have_rare(const double* recs, size_t words);
+
 // Kernel launchers (tp_track.cu, compiled once with and once without FMA
 // contraction).  Return a cudaError_t value.
 constexpr int kTrackMaxBlock = 128;  // launch bound of the tracking kernels
@@ -98,6 +103,7 @@ struct LatticeHost {
     int32_t sched_stride, sched_turn0, sched_nturns;
     bool has_schedule;
     int64_t nmis;
+    const tp_misalign* mis;   // nmis rows
 };
 void lattice_host(const tp_lattice* lat, LatticeHost* out);
 
@@ -112,7 +118,7 @@ struct CtxHost {
 };
 void ctx_host(const tp_ctx* c, CtxHost* out);
 tp_stats* ctx_stats(tp_ctx* c);
-constexpr int kCtxScratchSlots = 12;
+constexpr int kCtxScratchSlots = 16;
 int ctx_scratch(tp_ctx* c, int slot, size_t bytes, void** out);
 // The lattices of a batch in variant order.
 void batch_lattices(const tp_batch* b, std::vector<const tp_lattice*>* out);

@@ -621,6 +621,21 @@ static __device__ __noinline__ void lbend(P6& s, const double* w, const RecHdr& 
     edge_fringe(s, w[lb::IRHO], w[lb::FX_OUT], w[lb::E_OUT], w[lb::FC_OUT], 1, h.flags & RF_FC_OUT_ZERO, true);
 }
 
+// LorentzBoost / InvLorentzBoost (src/tracking.jl:1587-1606).
+__device__ __forceinline__ void lorentz_boost(P6& s, const double* w) {
+    const double ic = w[lor::A], ta = w[lor::B];
+    double x_new = s.x + ta * s.z;
+    double d_new = s.d - ta * s.px;
+    s.x = x_new; s.px = s.px * ic; s.py = s.py * ic; s.z = s.z * ic; s.d = d_new;
+}
+
+__device__ __forceinline__ void inv_lorentz_boost(P6& s, const double* w) {
+    const double ca = w[lor::A], sa = w[lor::B];
+    double x_new = s.x - sa * s.z;
+    double d_new = s.d + sa * s.px;
+    s.x = x_new; s.px = s.px * ca; s.py = s.py * ca; s.z = s.z * ca; s.d = d_new;
+}
+
 // StrongGaussianBeam (src/tracking.jl:1621-1641): the slice weights and
 // offsets follow the fixed words.
 static __device__ __noinline__ void strong_gauss(P6& s, const double* w) {
@@ -865,8 +880,37 @@ __device__ __forceinline__ void mis_exit(const MisalignDev& m, P6& s) {
     s.py = s.py + m.t2[3]; s.z = s.z + m.t2[4]; s.d = s.d + m.t2[5];
 }
 
-// One lattice entry.  Returns false for an unknown record kind.
+// The kinds outside the integrator core, out of line behind one call site.
 template <bool EXACT>
+static __device__ __noinline__ bool apply_rare(P6& s, const double* w, const RecHdr& h, double beti, double beta,
+                                               double beta2) {
+    switch (h.kind) {
+        case DK_SOLENOID: solenoid<EXACT>(s, w, beti); break;
+        case DK_CORRECTOR: corrector(s, w); break;
+        case DK_TRANSLATION: translation(s, w, beti); break;
+        case DK_YROTATION: yrotation(s, w, beti); break;
+        case DK_CRAB: crab_cavity<EXACT>(s, w, h, beti); break;
+        case DK_ACCEL: accel_cavity(s, w, beta2); break;
+        case DK_LONG_RF_MAP: long_rf_map(s, w, beta); break;
+        case DK_LORENTZ: lorentz_boost(s, w); break;
+        case DK_INV_LORENTZ: inv_lorentz_boost(s, w); break;
+        case DK_STRONG_THIN_GAUSS: strong_thin_gauss(s, w); break;
+        case DK_LBEND: lbend(s, w, h); break;
+        case DK_SGB: strong_gauss(s, w); break;
+        case DK_RLC_WAKE: rlc_wake(s, w); break;
+        case DK_TAB_WAKE: tab_wake(s, w, h); break;
+        case DK_WIGGLER: wiggler(s, w); break;
+        case DK_NAN: set_nan(s); break;
+        default: return false;
+    }
+    return true;
+}
+
+// One lattice entry.  Returns false for an unknown record kind.  RARE =
+// false drops the call of apply_rare (tables of core kinds only): the tracking
+// kernel is then the integrator core alone, which measured 2.5% faster on the
+// DBA ring than the same loop with the rare kinds' dispatch reachable.
+template <bool EXACT, bool RARE = true>
 __device__ __forceinline__ bool apply_record(P6& s, const double* rec, const RecHdr& h, const MisalignDev* mis,
                                              double beti, double beta, double beta2) {
     const double* w = rec + HDR_WORDS;
@@ -905,35 +949,9 @@ __device__ __forceinline__ bool apply_record(P6& s, const double* rec, const Rec
             break;
         case DK_EXACT_SBEND: exact_sbend(s, w, h, beti); break;
         case DK_RF: rf_cavity<EXACT>(s, w, h, beti, beta2); break;
-        case DK_SOLENOID: solenoid<EXACT>(s, w, beti); break;
-        case DK_CORRECTOR: corrector(s, w); break;
-        case DK_TRANSLATION: translation(s, w, beti); break;
-        case DK_YROTATION: yrotation(s, w, beti); break;
-        case DK_CRAB: crab_cavity<EXACT>(s, w, h, beti); break;
-        case DK_ACCEL: accel_cavity(s, w, beta2); break;
-        case DK_LONG_RF_MAP: long_rf_map(s, w, beta); break;
-        case DK_LORENTZ: {
-            const double ic = w[lor::A], ta = w[lor::B];
-            double x_new = s.x + ta * s.z;
-            double d_new = s.d - ta * s.px;
-            s.x = x_new; s.px = s.px * ic; s.py = s.py * ic; s.z = s.z * ic; s.d = d_new;
+        default:
+            if (!RARE || !apply_rare<EXACT>(s, w, h, beti, beta, beta2)) return false;
             break;
-        }
-        case DK_INV_LORENTZ: {
-            const double ca = w[lor::A], sa = w[lor::B];
-            double x_new = s.x - sa * s.z;
-            double d_new = s.d + sa * s.px;
-            s.x = x_new; s.px = s.px * ca; s.py = s.py * ca; s.z = s.z * ca; s.d = d_new;
-            break;
-        }
-        case DK_STRONG_THIN_GAUSS: strong_thin_gauss(s, w); break;
-        case DK_LBEND: lbend(s, w, h); break;
-        case DK_SGB: strong_gauss(s, w); break;
-        case DK_RLC_WAKE: rlc_wake(s, w); break;
-        case DK_TAB_WAKE: tab_wake(s, w, h); break;
-        case DK_WIGGLER: wiggler(s, w); break;
-        case DK_NAN: set_nan(s); break;
-        default: return false;
     }
     if (h.flags & RF_MISALIGN) mis_exit(mis[h.aux], s);
     return true;

@@ -105,6 +105,7 @@ TP_API int tp_ringpass_noalloc(const tp_lattice* lat, double* coords, int64_t n,
     a.table = scratch + kHeadWords;
     a.table_words = int32_t(v.words);
     a.nelem = v.nelem;
+    a.rare = tp::records_have_rare(v.program, v.words) ? 1 : 0;
     a.coords = coords;
     a.n = n;
     a.lost_flags = lost_flags;

@@ -623,16 +623,11 @@ __device__ __forceinline__ void rev_rf(P6& s, L6& l, const double* w, const RecH
     }
 }
 
-// Device kinds the reverse sweep implements.
-__host__ __device__ constexpr bool reverse_supported(int kind) {
-    return kind == DK_IDENTITY || kind == DK_DRIFT || kind == DK_MULTIPOLE || kind == DK_THIN || kind == DK_SBEND ||
-           kind == DK_EXACT_SBEND || kind == DK_RF;
-}
-
-// One lattice entry backwards.  pm: normal-coefficient slot of the strength
-// parameter of this entry (0 = not a parameter); g accumulates d/d pb_pm.
+// The integrator kinds backwards (the body of a record, without its
+// misalignment).  pm: normal-coefficient slot of the strength parameter of
+// this entry (0 = not a parameter); g accumulates d/d pb_pm.
 template <bool EXACT>
-__device__ __forceinline__ bool reverse_record(P6& s, L6& l, const double* rec, const RecHdr& h, double beti,
+__device__ __forceinline__ bool reverse_core(P6& s, L6& l, const double* rec, const RecHdr& h, double beti,
                                                double beta2, int pm, double& g) {
     const double* w = rec + HDR_WORDS;
     switch (h.kind) {

@@ -130,6 +130,7 @@ struct tp_batch {
     std::vector<int32_t> h_nelem;
     std::vector<int64_t> h_mis_off;    // misalignment row offset per variant
     size_t table_words = 0;
+    bool rare = false;         // some variant holds kinds outside the integrator core
     double* sched = nullptr;           // concatenated per-turn schedule tables
     int64_t* sched_v = nullptr;        // per variant: word offset (-1: none), stride, first turn, turns
     std::vector<uint64_t> h_ver;       // lattice versions the device tables were built from
@@ -371,6 +372,7 @@ void lattice_host(const tp_lattice* lat, LatticeHost* out) {
     out->sched_turn0 = lat->sturn0;
     out->sched_nturns = lat->snturns;
     out->nmis = int64_t(lat->mis.size());
+    out->mis = lat->mis.data();
 }
 
 void ctx_host(const tp_ctx* c, CtxHost* out) {
@@ -703,6 +705,7 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     a.sched_turn0 = L->sturn0;
     a.sched_nturns = L->snturns;
     a.mis = dl.mis;
+    a.rare = records_have_rare(L->program.data(), L->program.size()) ? 1 : 0;
     a.coords = d_coords;
     a.n = n;
     a.lost_flags = d_lost;
@@ -852,6 +855,8 @@ static int batch_build(tp_batch* b) {
         int32_t mbase = int32_t(mis.size());
         size_t at = table.size();
         table.insert(table.end(), L->program.begin(), L->program.end());
+        if (v == 0) b->rare = false;
+        if (records_have_rare(L->program.data(), L->program.size())) b->rare = true;
         if (mbase > 0) {  // shift misalignment rows of this variant
             for (size_t e = 0; e < L->elems.size(); ++e) {
                 RecHdr* h = reinterpret_cast<RecHdr*>(table.data() + at + L->rec_off[e]);
@@ -1050,6 +1055,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     a.table = b->table;
     a.table_words = int32_t(b->table_words);
     a.mis = b->mis;
+    a.rare = b->rare ? 1 : 0;
     a.coords = d_coords;
     a.n = n;
     a.lost_flags = d_lost;

@@ -129,7 +129,7 @@ __device__ __forceinline__ const double* resolve(const double* rec, RecHdr& h, c
 // Track the particles of one warp through `nturns` turns of the table `tab`
 // (`nelem` records).  Slot state is per lane.  With REFILL, lanes take new
 // particles from `next_particle` at turn boundaries until it returns < 0.
-template <bool EXACT, bool REFILL, typename NextFn>
+template <bool EXACT, bool REFILL, bool RARE, typename NextFn>
 __device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, double beti, NextFn next_particle) {
     const double beta = 1.0 / beti;
     const double beta2 = beta * beta;
@@ -177,7 +177,7 @@ __device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, doubl
                     act = false;
                 } else {
                     P6 sn = s;
-                    if (!apply_record<EXACT>(sn, r, h, a.mis, beti, beta, beta2)) {
+                    if (!apply_record<EXACT, RARE>(sn, r, h, a.mis, beti, beta, beta2)) {
                         atomicOr(a.err, DE_BAD_KIND);
                         act = false;
                     } else if (is_lost(sn, a.limx, a.limy)) {
@@ -205,7 +205,7 @@ __device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, doubl
     }
 }
 
-template <bool EXACT, bool REFILL>
+template <bool EXACT, bool REFILL, bool RARE>
 __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_single(TrackArgs a) {
     extern __shared__ __align__(16) double smem[];
     __shared__ __align__(8) uint64_t mbar;
@@ -228,14 +228,14 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_single(TrackAr
             unsigned long long j = base + __popc(need & ((1u << lane) - 1u));
             return j < (unsigned long long)a.n ? int64_t(j) : -1;
         };
-        run_warp<EXACT, true>(a, tab, a.nelem, a.beti, next);
+        run_warp<EXACT, true, RARE>(a, tab, a.nelem, a.beti, next);
     } else {
         const int64_t gid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
         auto next = [&](unsigned need, int lane, bool& more) -> int64_t {
             more = false;
             return gid < a.n ? gid : -1;
         };
-        run_warp<EXACT, false>(a, tab, a.nelem, a.beti, next);
+        run_warp<EXACT, false, RARE>(a, tab, a.nelem, a.beti, next);
     }
 }
 
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_single(TrackAr
 // refills lanes freed by a loss at turn boundaries until the pool is empty;
 // later tiles of an emptied variant end at once.  Either way every particle is
 // tracked from turn 0 with its own turn counter, so the results are the same.
-template <bool EXACT, bool REFILL>
+template <bool EXACT, bool REFILL, bool RARE>
 __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_batched(TrackArgs a, const int64_t* tile_off) {
     const int lane = threadIdx.x & 31;
     const int64_t ntiles = tile_off[a.nvar];
@@ -290,49 +290,53 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_batched(TrackA
             av.sched_stride = int32_t(a.sched_v[4 * v + 1]);
             av.sched_turn0 = int32_t(a.sched_v[4 * v + 2]);
             av.sched_nturns = int32_t(a.sched_v[4 * v + 3]);
-            run_warp<EXACT, REFILL>(av, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next);
+            run_warp<EXACT, REFILL, RARE>(av, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next);
         } else {
-            run_warp<EXACT, REFILL>(a, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next);
+            run_warp<EXACT, REFILL, RARE>(a, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next);
         }
     }
 }
 
-static size_t smem_bytes(const TrackArgs& a) { return size_t(a.smem_words) * 8; }
+// The kernel instance of (exact drift, refill, rare kinds) chosen at run time.
+template <bool EXACT, bool REFILL, bool RARE>
+int launch_t(const TrackArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
+    if (a.nvar > 0) {
+        const int64_t* tile_off = a.toff + (a.nvar + 1);  // host packs tile offsets and the order after toff
+        track_batched<EXACT, REFILL, RARE><<<grid, block, 0, st>>>(a, tile_off);
+        return int(cudaGetLastError());
+    }
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(track_single<EXACT, REFILL, RARE>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        if (e != cudaSuccess) return int(e);
+    }
+    track_single<EXACT, REFILL, RARE><<<grid, block, smem, st>>>(a);
+    return int(cudaGetLastError());
+}
+
+template <bool EXACT, bool REFILL>
+int launch_r(const TrackArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
+    return a.rare ? launch_t<EXACT, REFILL, true>(a, grid, block, smem, st)
+                  : launch_t<EXACT, REFILL, false>(a, grid, block, smem, st);
+}
 
 int launch(const TrackArgs& a, int grid, int block, int ppt, size_t smem, void* stream) {
     (void)ppt;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    if (a.nvar > 0) {
-        const int64_t* tile_off = a.toff + (a.nvar + 1);  // host packs tile offsets and the order after toff
-        if (a.exact && a.refill) track_batched<true, true><<<grid, block, 0, st>>>(a, tile_off);
-        else if (a.exact) track_batched<true, false><<<grid, block, 0, st>>>(a, tile_off);
-        else if (a.refill) track_batched<false, true><<<grid, block, 0, st>>>(a, tile_off);
-        else track_batched<false, false><<<grid, block, 0, st>>>(a, tile_off);
-        return int(cudaGetLastError());
-    }
-    (void)smem_bytes;
-    if (smem > 48 * 1024) {
-        cudaError_t e;
-        if (a.exact && a.refill) e = cudaFuncSetAttribute(track_single<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        else if (a.exact) e = cudaFuncSetAttribute(track_single<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        else if (a.refill) e = cudaFuncSetAttribute(track_single<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        else e = cudaFuncSetAttribute(track_single<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
-        if (e != cudaSuccess) return int(e);
-    }
-    if (a.exact && a.refill) track_single<true, true><<<grid, block, smem, st>>>(a);
-    else if (a.exact) track_single<true, false><<<grid, block, smem, st>>>(a);
-    else if (a.refill) track_single<false, true><<<grid, block, smem, st>>>(a);
-    else track_single<false, false><<<grid, block, smem, st>>>(a);
-    return int(cudaGetLastError());
+    if (a.nvar > 0) smem = 0;
+    if (a.exact && a.refill) return launch_r<true, true>(a, grid, block, smem, st);
+    if (a.exact) return launch_r<true, false>(a, grid, block, smem, st);
+    if (a.refill) return launch_r<false, true>(a, grid, block, smem, st);
+    return launch_r<false, false>(a, grid, block, smem, st);
 }
 
 int occupancy(int block, int ppt, size_t smem, int* blocks_per_sm) {
     (void)ppt;
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(track_single<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaError_t e = cudaFuncSetAttribute(track_single<true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return int(e);
     }
-    return int(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, track_single<true, true>, block, smem));
+    return int(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, track_single<true, true, false>, block, smem));
 }
 
 }  // namespace TP_NS

@@ -15,14 +15,56 @@ import numpy as np
 from . import tracking
 
 
-def one_turn_map(lat, beam, reference=None, nturns=1):
-    """6x6 one-turn map about `reference` (default zeros), exact tangent map
-    (the reference: central differences with h = 1e-8)."""
+def one_turn_map(lat, beam, reference=None, nturns=1, method="exact", h=1e-8):
+    """6x6 one-turn map about `reference` (default zeros).
+
+    method="exact": the exact tangent map of the tracked maps (device reverse
+    sweep).  method="fd": the reference's own estimate (src/optics.jl:110-121),
+    central differences (linepass(r + h e_i) - linepass(r - h e_i)) / 2h, with
+    the 12 orbits tracked in one device call; since the tracking is
+    bit-identical to the reference's maps, so is this matrix."""
     ref = np.zeros(6) if reference is None else np.asarray(reference, dtype=np.float64).reshape(6)
+    if method == "fd":
+        return _fd_map(lat, beam, ref, nturns, h)
+    if method != "exact":
+        raise ValueError("method must be 'exact' or 'fd'")
     M, _ = tracking.one_turn_jacobian(lat, beam, ref[None, :], nturns=nturns)
     if np.isnan(M[0]).any():
         raise ValueError("the reference orbit is lost within the turn")
     return M[0]
+
+
+def fd_orbits(reference, h=1e-8):
+    """The 12 orbits of the central-difference map: rows 2i, 2i+1 are
+    reference + h e_i and reference - h e_i."""
+    ref = np.asarray(reference, dtype=np.float64).reshape(6)
+    out = np.empty((12, 6), dtype=np.float64, order="F")
+    for i in range(6):
+        e = np.zeros(6)
+        e[i] = 1.0
+        out[2 * i] = ref + h * e
+        out[2 * i + 1] = ref - h * e
+    return out
+
+
+def fd_assemble(tracked, h=1e-8):
+    """M[:, i] = (rp_i - rm_i) / (2h) from the tracked `fd_orbits`."""
+    M = np.empty((6, 6))
+    for i in range(6):
+        M[:, i] = (tracked[2 * i] - tracked[2 * i + 1]) / (2.0 * h)
+    return M
+
+
+def _fd_map(lat, beam, ref, nturns, h):
+    c = fd_orbits(ref, h)
+    lost = np.zeros(12, np.int64)
+    if nturns == 1:
+        tracking.linepass_(c, lat, beam, lost)
+    else:
+        tracking.ringpass_(c, lat, beam, lost, nturns)
+    if lost.any():
+        raise ValueError("the reference orbit is lost within the turn")
+    return fd_assemble(c, h)
 
 
 def one_turn_maps(lat, beam, references, nturns=1):
