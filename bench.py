@@ -51,7 +51,10 @@ def parse():
     p.add_argument("--steps", type=int, default=10)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--workload", default="dba", choices=["dba", "fodo", "batched", "adjoint", "batched_adjoint"])
+    p.add_argument("--workload", default="dba", choices=["dba", "fodo", "batched", "adjoint", "batched_adjoint",
+                                                         "tpsa"])
+    p.add_argument("--order", type=int, default=4, help="tpsa workload: series order")
+    p.add_argument("--maps", type=int, default=0, help="tpsa workload: maps per step (0: default)")
     p.add_argument("--n-gauss", type=int, default=1 << 20)
     p.add_argument("--grid", type=int, default=512)
     p.add_argument("--turns", type=int, default=0, help="turns per step (0: the workload's default)")
@@ -566,6 +569,83 @@ def main_batched_adjoint(args, tp, torch, rank, world, local, dist):
         print(json.dumps(line))
 
 
+# ---------------------------------------------------------------------------
+# Truncated power series maps
+# ---------------------------------------------------------------------------
+def main_tpsa(args, tp, torch, rank, world, local, dist):
+    """TPSA maps (ext/TrackPadPolySeriesExt.jl) of the FODO ring about seeded
+    reference orbits: each step tracks `maps` series maps of order `order`
+    through `turns` turns with host arrays in and out (tp_tpsa_ringpass)."""
+    import trackpad_b200.workloads as W
+    lat, beam = W.fodo_ring(), W.fodo_beam()
+    nmaps = args.maps or 2048
+    order = args.order
+    turns = args.turns or 1
+    refs = W.gaussian(nmaps, seed=100 + rank, sigma=(1e-4, 1e-5, 1e-4, 1e-5, 1e-3, 1e-4))
+    base = np.ascontiguousarray(np.stack([tp.polyseries_variables(r, order).coef for r in refs]))
+    m = base.shape[2]
+    for _ in range(args.warmup):
+        tp.tpsa.ringpass(lat, base, beam, turns, order=order)
+    if dist:
+        dist.barrier()
+    clocks = Clocks(local)
+    k_ms, wall, flops, smul = [], [], 0.0, 0.0
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        out = tp.tpsa.ringpass(lat, base, beam, turns, order=order)
+        wall.append(time.perf_counter() - t0)
+        st = tp.tpsa.last_stats()
+        k_ms.append(st["kernel_ms"])
+        flops += st["flops"]
+        smul += st["series_mul"]
+    clk = clocks.stop()
+    units = float(nmaps) * len(lat) * turns
+    t = torch.tensor([float(np.sum(k_ms)) * 1e-3, float(np.sum(wall))], dtype=torch.float64,
+                     device=torch.device("cuda", local))
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    kern_s, wall_s = float(t[0]), float(t[1])
+    peak = tp.probe_fp64_peak(local)
+    achieved = flops / kern_s / 1e12
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        import oracle_ref
+        nsamp, dt = 0, 0.0
+        while dt < 10.0 and nsamp < nmaps:
+            k = min(8, nmaps - nsamp)
+            arr = np.ascontiguousarray(base[nsamp:nsamp + k])
+            t0 = time.perf_counter()
+            oracle_ref.tpsa_ringpass(lat, arr, tp.beti(beam), order, nturns=turns)
+            dt += time.perf_counter() - t0
+            nsamp += k
+        cpu = {"value": nsamp * len(lat) * turns / dt, "unit": "map*element*turns/s", "cores": 1, "kind": "port",
+               "sample": f"{nsamp} of the step's maps through the oracle's series algebra, one thread, {dt:.1f} s"}
+    if rank == 0:
+        line = {
+            "metric": f"TPSA map*element*turns/s (order {order})", "value": units * world * args.steps / kern_s,
+            "unit": "map*element*turns/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": kern_s / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox reference orbits)",
+            "config": {"workload": f"FODO ring, 8 cells (32 elements), 1 GeV e-, {nmaps} maps of order {order} "
+                                   f"({m} coefficients per series), {turns} turn(s) per step",
+                       "maps_per_gpu": nmaps, "order": order, "coefficients": m,
+                       "series_products_per_step": smul / args.steps,
+                       "launch": {"grid": st["grid"], "block": st["block"], "shared_pool": st["shared_pool"],
+                                  "slots": st["slots"], "slots_used": st["slots_used"]},
+                       "l2": "inputs and outputs cross PCIe every step (host arrays)"},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "flops_per_launch": flops / args.steps, "kernel_ms": kern_s / args.steps * 1e3,
+                         "peak_source": "measured FP64 FMA throughput of this device (tp_probe_fp64_peak)"},
+            "cpu_baseline": cpu,
+            "e2e": {"value": units * world * args.steps / wall_s, "unit": "map*element*turns/s",
+                    "h2d_bytes_per_step": int(base.nbytes), "d2h_bytes_per_step": int(base.nbytes)},
+            "gpu_launches": args.steps, "clocks": clk,
+        }
+        print(json.dumps(line))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -581,7 +661,7 @@ def main():
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
     fn = {"dba": main_track, "fodo": main_track, "batched": main_batched, "adjoint": main_adjoint,
-          "batched_adjoint": main_batched_adjoint}[args.workload]
+          "batched_adjoint": main_batched_adjoint, "tpsa": main_tpsa}[args.workload]
     fn(args, tp, torch, rank, world, local, dist)
     if dist:
         dist.barrier()

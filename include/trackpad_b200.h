@@ -432,6 +432,44 @@ TP_API int tp_ringpass_noalloc(const tp_lattice* lat, double* coords, int64_t n,
                                int32_t turn0, double aperture_x, double aperture_y, void* stream);
 
 /* ------------------------------------------------------------------------- */
+/* Truncated power series (TPSA) maps                                         */
+/* ------------------------------------------------------------------------- */
+/* linepass / ringpass of six CTPS values and polyseries_one_turn_map
+ * (ext/TrackPadPolySeriesExt.jl:654-705; CTPS is the truncated power series
+ * type of the PolySeries package).  A map is six series (x, px, y, py, z,
+ * delta) in the six phase-space variables truncated at total order `order`
+ * (0..10), each stored as M = C(order + 6, 6) coefficients in the order
+ * tp_tpsa_monomials gives: by degree, then by exponent vector in descending
+ * lexicographic order.  polyseries_variables(x0) is the map with constant
+ * parts x0 and unit first-order parts. */
+TP_API int tp_tpsa_coefficients(int32_t order, int64_t* ncoef);
+/* exps: M x 6 exponents of the monomials, in coefficient order. */
+TP_API int tp_tpsa_monomials(int32_t order, int32_t* exps);
+/* maps: host array of nmaps x 6 x M doubles, updated in place by nturns
+ * passes of the lattice from turn turn0 (per-turn schedules apply).  Element
+ * kinds without a CTPS pass! method in the reference (ExactSBend, LBend,
+ * Wiggler) give TP_EUNSUPPORTED; no aperture or loss check (as the
+ * reference). */
+TP_API int tp_tpsa_ringpass(tp_ctx* ctx, const tp_lattice* lat, double* maps, int64_t nmaps, int32_t order,
+                            double beti, int32_t nturns, int32_t turn0);
+/* Work of the last tp_tpsa_ringpass on this thread: series products (each
+ * `pairs` coefficient products), elementwise series operations (M
+ * coefficients each), their FLOPs (a product counts 2*pairs - M), and the
+ * kernel's device time. */
+typedef struct tp_tpsa_stats {
+    int64_t maps;
+    int32_t order, coefficients;
+    int64_t pairs;
+    double series_mul, series_lin, flops;
+    double kernel_ms;
+    int32_t grid, block, shared_pool;
+    int32_t slots;                /* series slots per map in the pool           */
+    int32_t slots_used;           /* most series slots one map held at a time */
+    int32_t reserved;
+} tp_tpsa_stats;
+TP_API int tp_tpsa_last_stats(tp_tpsa_stats* out);
+
+/* ------------------------------------------------------------------------- */
 /* Diagnostics                                                                */
 /* ------------------------------------------------------------------------- */
 /* Measured FP64 fused-multiply-add throughput of the device (TFLOP/s, 2 FLOPs

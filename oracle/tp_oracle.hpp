@@ -29,6 +29,7 @@
 #include <cstdint>
 #include <cstring>
 #include <limits>
+#include <type_traits>
 #include <vector>
 
 #include "../include/trackpad_b200.h"
@@ -66,6 +67,13 @@ inline double exp(double x) { return tp::libm::exp(x); }
 inline double expm1(double x) { return tp::libm::expm1(x); }
 inline double sinh(double x) { return tp::libm::sinh(x); }
 inline double cosh(double x) { return tp::libm::cosh(x); }
+
+// Truncated power series (tp_tpsa_oracle.hpp) specialise this: the TPSA
+// extension (ext/TrackPadPolySeriesExt.jl) tracks with the same pass! bodies
+// except for an always-exact drift, bend edges whose fy uses the constant
+// parts of delta and px, and wakes evaluated at the constant part of z.
+template <class T>
+struct is_tps : std::false_type {};
 
 template <class T>
 struct V6 {
@@ -178,6 +186,16 @@ inline V6<T> exit_(const Elem<T>& e, V6<T> r) {
 template <class T>
 inline V6<T> drift6(const V6<T>& r, T L, T beti, bool exact) {
     using std::sqrt;
+    if constexpr (is_tps<T>::value) {
+        // drift6_tpsa (ext/TrackPadPolySeriesExt.jl:57-65): exact, no loss
+        // check; L / sqrt(pz2) as L * pz2^(-1/2) (one series)
+        T pz2 = T(1.0) + T(2.0) * r[5] * beti + r[5] * r[5] - r[1] * r[1] - r[3] * r[3];
+        T NormL = L * rsqrt(pz2);
+        T x_new = r[0] + NormL * r[1];
+        T y_new = r[2] + NormL * r[3];
+        T z_new = r[4] + NormL * (beti + r[5]) - L * beti;
+        return V6<T>{{x_new, r[1], y_new, r[3], z_new, r[5]}};
+    }
     if (exact) {
         T pz2 = T(1.0) + T(2.0) * r[5] * beti + r[5] * r[5] - r[1] * r[1] - r[3] * r[3];
         if (value_of(pz2) <= 0.0) return nan6<T>();
@@ -215,6 +233,20 @@ inline V6<T> edge_fringe(const V6<T>& r, T inv_rho, T edge_angle, T fint, T gap,
         T sedge = sin(edge_angle);
         T cedge = cos(edge_angle);
         fringecorr = inv_rho * gap * fint * (T(1.0) + sedge * sedge) / cedge;
+    }
+    if constexpr (is_tps<T>::value) {
+        // edge_fringe_entrance_tpsa / _exit_tpsa (ext/TrackPadPolySeriesExt.jl:161-215):
+        // fx and fy are numbers, fy from the constant parts of delta and px
+        const double ir = value_of(inv_rho), ea = value_of(edge_angle), fc = value_of(fringecorr);
+        const double d0 = value_of(r[5]), px0 = value_of(r[1]);
+        const double fxd = ir * tp::libm::tan(ea);
+        double fyd;
+        if (method == 2) fyd = ir * tp::libm::tan(ea - fc / (1.0 + d0)) / (1.0 + d0);
+        else if (method == 3) fyd = ir * tp::libm::tan(is_exit ? (ea - fc - px0 / (1.0 + d0)) : (ea - fc + px0 / (1.0 + d0)));
+        else fyd = ir * tp::libm::tan(ea - fc / (1.0 + d0));
+        T px_new = r[1] + r[0] * T(fxd);
+        T py_new = r[3] - r[2] * T(fyd);
+        return V6<T>{{r[0], px_new, r[2], py_new, r[4], r[5]}};
     }
     T fx = inv_rho * tan(edge_angle);
     T fy;
@@ -848,6 +880,14 @@ template <class T>
 inline V6<T> pass_rlc_wake(const Elem<T>& e, const V6<T>& r) {
     using std::sqrt;
     if (value_of(e.param[3]) == 0.0) return r;
+    if constexpr (is_tps<T>::value) {
+        // ext/TrackPadPolySeriesExt.jl:630-639: the wake at the constant part of z
+        Elem<double> ed;
+        for (int i = 0; i < 4; ++i) ed.param[i] = value_of(e.param[i]);
+        V6<double> rd{{0.0, 0.0, 0.0, 0.0, value_of(r[4]), 0.0}};
+        const double dd = pass_rlc_wake(ed, rd)[5];  // -scale * W(t)
+        return V6<T>{{r[0], r[1], r[2], r[3], r[4], r[5] + T(dd)}};
+    }
     T zc = r[4] / T(C_LIGHT);
     T t = is_nan(zc) ? zc : (value_of(zc) > 0.0 ? T(0.0) : zc);  // min(z/c, 0), NaN propagates
     T Q0 = e.param[2];
@@ -868,6 +908,16 @@ inline V6<T> pass_rlc_wake(const Elem<T>& e, const V6<T>& r) {
 template <class T>
 inline V6<T> pass_tab_wake(const Elem<T>& e, const V6<T>& r) {
     if (value_of(e.param[1]) == 0.0) return r;
+    if constexpr (is_tps<T>::value) {
+        // ext/TrackPadPolySeriesExt.jl:641-649: the wake at the constant part of z
+        Elem<double> ed;
+        ed.aux = e.aux;
+        ed.iparam[1] = e.iparam[1];
+        for (int i = 0; i < 2; ++i) ed.param[i] = value_of(e.param[i]);
+        V6<double> rd{{0.0, 0.0, 0.0, 0.0, value_of(r[4]), 0.0}};
+        const double dd = pass_tab_wake(ed, rd)[5];
+        return V6<T>{{r[0], r[1], r[2], r[3], r[4], r[5] + T(dd)}};
+    }
     const int n = e.iparam[1] / 2;
     const double* xs = e.aux;
     const double* ys = e.aux + n;

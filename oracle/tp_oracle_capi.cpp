@@ -15,9 +15,11 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <string>
 #include <vector>
 
 #include "tp_oracle.hpp"
+#include "tp_tpsa_oracle.hpp"
 
 // ---------------------------------------------------------------------------
 // Op-counting scalar: the algorithmic FLOP table.  Rules: add/sub/mul/div/sqrt
@@ -103,6 +105,7 @@ struct Inputs {
 // Array fields of the elements of the next calls (tp_lattice_create_ex's aux),
 // set by orc_set_aux.
 std::vector<double> g_aux;
+std::string g_tpsa_error;  // message of the last failed TPSA call
 
 Lattice build_lattice(const Inputs& in) {
     Lattice lat;
@@ -350,5 +353,79 @@ int orc_submap(int32_t which, double* r6, double a0, double a1, double beti) {
     for (int c = 0; c < 6; ++c) r6[c] = r[c];
     return 0;
 }
+
+// ---------------------------------------------------------------------------
+// TPSA (ext/TrackPadPolySeriesExt.jl): series of order `order` in the six
+// variables; maps are nmaps x 6 x M coefficients (M = C(order + 6, 6)).
+// ---------------------------------------------------------------------------
+int orc_tpsa_set_order(int32_t order) {
+    if (order < 0 || order > 10) return -1;
+    tps_set_order(order);
+    return tps_desc().M;
+}
+
+// Exponent vectors of the monomials (M x 6), in coefficient order.
+int orc_tpsa_monomials(int32_t* exps) {
+    const TpsDesc& d = tps_desc();
+    for (int k = 0; k < d.M; ++k)
+        for (int v = 0; v < 6; ++v) exps[k * 6 + v] = d.mono[size_t(k)][size_t(v)];
+    return d.M;
+}
+
+// One series operation on full series a, b (M coefficients each): op 0 a*b,
+// 1 a/b, 2 inv(a), 3 sqrt(a), 4 a^(-1/2), 5 exp(a), 6 sin(a), 7 cos(a).
+int orc_tpsa_op(int32_t op, const double* a, const double* b, double* out) {
+    const int M = tps_desc().M;
+    Tps A = Tps::full(), B = Tps::full();
+    for (int k = 0; k < M; ++k) { A.c[size_t(k)] = a[k]; if (b) B.c[size_t(k)] = b[k]; }
+    Tps R;
+    switch (op) {
+        case 0: R = A * B; break;
+        case 1: R = A / B; break;
+        case 2: R = inv(A); break;
+        case 3: R = sqrt(A); break;
+        case 4: R = rsqrt(A); break;
+        case 5: R = exp(A); break;
+        case 6: R = sin(A); break;
+        case 7: R = cos(A); break;
+        default: return -1;
+    }
+    for (int k = 0; k < M; ++k) out[k] = R.is_const() ? (k == 0 ? R.c[0] : 0.0) : R.c[size_t(k)];
+    return 0;
+}
+
+// linepass / ringpass of series maps (ext/TrackPadPolySeriesExt.jl:654-686):
+// nturns passes from turn turn0, elements resolved per turn from the schedule.
+// Returns -2 for an element kind without a TPSA pass! method.
+int orc_tpsa_ringpass(const tp_elem* elems, int64_t ne, const tp_misalign* mis, int64_t nmis,
+                      const int32_t* sfields, int32_t nfields, int32_t sturn0, int32_t snturns,
+                      const double* svalues, double* maps, int64_t nmaps, double beti, int32_t nturns,
+                      int32_t turn0) {
+    for (int64_t e = 0; e < ne; ++e)
+        if (!tpsa_supported(elems[e].kind)) return -2;
+    Inputs in{elems, ne, mis, nmis, sfields, nfields, sturn0, snturns, svalues};
+    Lattice lat = build_lattice(in);
+    const int M = tps_desc().M;
+    try {
+    for (int64_t m = 0; m < nmaps; ++m) {
+        V6<Tps> r;
+        for (int c = 0; c < 6; ++c) {
+            r[c] = Tps::full();
+            for (int k = 0; k < M; ++k) r[c].c[size_t(k)] = maps[(m * 6 + c) * M + k];
+        }
+        for (int32_t t = 0; t < nturns; ++t)
+            for (int64_t e = 0; e < ne; ++e) r = tpsa_pass(elem_at<Tps>(lat, e, turn0 + t), r, Tps(beti));
+        for (int c = 0; c < 6; ++c)
+            for (int k = 0; k < M; ++k)
+                maps[(m * 6 + c) * M + k] = r[c].is_const() ? (k == 0 ? r[c].c[0] : 0.0) : r[c].c[size_t(k)];
+    }
+    } catch (const std::exception& ex) {
+        g_tpsa_error = ex.what();
+        return -3;
+    }
+    return 0;
+}
+
+const char* orc_tpsa_error(void) { return g_tpsa_error.c_str(); }
 
 }  // extern "C"

@@ -36,6 +36,12 @@ def lib():
         _lib.orc_submap.argtypes = [C.c_int32, P, C.c_double, C.c_double, C.c_double]
         _lib.orc_max_threads.restype = C.c_int
         _lib.orc_set_aux.argtypes = [P, C.c_int64]
+        _lib.orc_tpsa_set_order.argtypes = [C.c_int32]
+        _lib.orc_tpsa_monomials.argtypes = [P]
+        _lib.orc_tpsa_op.argtypes = [C.c_int32, P, P, P]
+        _lib.orc_tpsa_ringpass.argtypes = [P, C.c_int64, P, C.c_int64, P, C.c_int32, C.c_int32, C.c_int32, P, P,
+                                           C.c_int64, C.c_double, C.c_int32, C.c_int32]
+        _lib.orc_tpsa_error.restype = C.c_char_p
     return _lib
 
 
@@ -138,3 +144,54 @@ def symplectic_error(M):
     """||M^T J M - J||_max with J = diag(J2, J2, -J2): in the reference's
     coordinates z is conjugate to delta with the sign of -c*dt."""
     return float(np.abs(M.T @ SYMPLECTIC_J @ M - SYMPLECTIC_J).max())
+
+
+# ---------------------------------------------------------------------------
+# TPSA (truncated power series) oracle
+# ---------------------------------------------------------------------------
+TPSA_OPS = {"mul": 0, "div": 1, "inv": 2, "sqrt": 3, "rsqrt": 4, "exp": 5, "sin": 6, "cos": 7}
+
+
+def tpsa_set_order(order):
+    """Set the series order; returns M, the number of coefficients."""
+    m = lib().orc_tpsa_set_order(int(order))
+    assert m > 0
+    return m
+
+
+def tpsa_monomials(order):
+    m = tpsa_set_order(order)
+    e = np.zeros((m, 6), np.int32)
+    lib().orc_tpsa_monomials(_ptr(e))
+    return e
+
+
+def tpsa_op(op, a, b=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    out = np.zeros_like(a)
+    bb = None if b is None else np.ascontiguousarray(b, dtype=np.float64)
+    assert lib().orc_tpsa_op(TPSA_OPS[op], _ptr(a), _ptr(bb), _ptr(out)) == 0
+    return out
+
+
+def tpsa_variables(x0, order):
+    """(6, M) coefficients of the six variables about x0 (CTPS(x0[i], i))."""
+    m = tpsa_set_order(order)
+    r = np.zeros((6, m))
+    for i in range(6):
+        r[i, 0] = x0[i]
+        r[i, 1 + i] = 1.0
+    return r
+
+
+def tpsa_ringpass(lat, maps, beti, order, nturns=1, turn0=0, sched=None):
+    """Series maps (nmaps, 6, M) through nturns passes, in place; returns the status."""
+    tpsa_set_order(order)
+    arr, n, mis, nm = _packed(lat)
+    f, nf, st0, snt, sv = _schedule(sched)
+    assert maps.flags.c_contiguous and maps.dtype == np.float64
+    st = lib().orc_tpsa_ringpass(arr, n, mis, nm, _ptr(f), nf, st0, snt, _ptr(sv), _ptr(maps),
+                                 maps.shape[0], beti, int(nturns), int(turn0))
+    if st == -3:
+        raise RuntimeError(lib().orc_tpsa_error().decode())
+    return st

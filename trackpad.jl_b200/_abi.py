@@ -128,6 +128,13 @@ def elem_array_aux(dicts):
 
 
 P = C.c_void_p
+class TpTpsaStats(C.Structure):
+    _fields_ = [("maps", C.c_int64), ("order", C.c_int32), ("coefficients", C.c_int32), ("pairs", C.c_int64),
+                ("series_mul", C.c_double), ("series_lin", C.c_double), ("flops", C.c_double),
+                ("kernel_ms", C.c_double), ("grid", C.c_int32), ("block", C.c_int32), ("shared_pool", C.c_int32),
+                ("slots", C.c_int32), ("slots_used", C.c_int32), ("reserved", C.c_int32)]
+
+
 _SIGS = {
     "tp_abi_version": (C.c_int, []),
     "tp_strerror": (C.c_char_p, [C.c_int]),
@@ -159,6 +166,10 @@ _SIGS = {
     "tp_probe_fp64_peak": (C.c_int, [P, C.POINTER(C.c_double)]),
     "tp_ringpass_noalloc": (C.c_int, [P, P, C.c_int64, P, P, P, C.c_double, C.c_int32, C.c_int32, C.c_double,
                                       C.c_double, P]),
+    "tp_tpsa_coefficients": (C.c_int, [C.c_int32, C.POINTER(C.c_int64)]),
+    "tp_tpsa_monomials": (C.c_int, [C.c_int32, P]),
+    "tp_tpsa_ringpass": (C.c_int, [P, P, P, C.c_int64, C.c_int32, C.c_double, C.c_int32, C.c_int32]),
+    "tp_tpsa_last_stats": (C.c_int, [C.POINTER(TpTpsaStats)]),
 }
 
 _lib = None

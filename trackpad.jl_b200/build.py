@@ -47,6 +47,7 @@ def build(verbose=False, ptxas_info=False):
         ("tp_adjoint.o", "tp_adjoint.cu", ["-fmad=false"]),
         ("tp_compile.o", "tp_compile.cpp", ["-fmad=false", "-x", "cu"]),
         ("tp_noalloc.o", "tp_noalloc.cu", ["-fmad=false"]),
+        ("tp_tpsa.o", "tp_tpsa.cu", ["-fmad=false"]),
     ]
     objs = []
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]

@@ -296,4 +296,36 @@ function tangent_maps(lat::Lattice, beam::Beam{Float64}, orbits::Matrix{Float64}
     [reshape(jac[:, i], 6, 6) for i in 1:n], err
 end
 
+"""
+    taylor_maps(lat, beam, r0s; order = 1, nturns = 1, turn = 0) -> (coef, exps)
+
+Truncated power series maps of `nturns` passes about each row of `r0s`
+(`n x 6`): the device counterpart of `polyseries_one_turn_map`
+(ext/TrackPadPolySeriesExt.jl:701-705) for many reference orbits at once.
+`coef[k, c, i]` is the coefficient of monomial k (exponents `exps[:, k]`) in
+component c of map i; a PolySeries CTPS is filled from it by exponents.
+"""
+function taylor_maps(lat::Lattice, beam::Beam{Float64}, r0s::Matrix{Float64}; order::Int = 1, nturns::Int = 1,
+                     turn::Integer = 0)
+    d = DeviceLattice(lat)
+    set_schedule!(d, lat, 0.0, 0.0, turn, max(nturns, 1))
+    m = Ref{Int64}(0)
+    check(ccall((:tp_tpsa_coefficients, LIB), Cint, (Int32, Ref{Int64}), order, m), "tp_tpsa_coefficients")
+    M = Int(m[])
+    exps = zeros(Int32, 6, M)
+    check(ccall((:tp_tpsa_monomials, LIB), Cint, (Int32, Ptr{Int32}), order, exps), "tp_tpsa_monomials")
+    n = size(r0s, 1)
+    coef = zeros(M, 6, n)                       # the C layout nmaps x 6 x M, column-major here
+    for i in 1:n, c in 1:6
+        coef[1, c, i] = r0s[i, c]
+        coef[1 + c, c, i] = 1.0                 # CTPS(r0[c], c)
+    end
+    GC.@preserve coef begin
+        check(ccall((:tp_tpsa_ringpass, LIB), Cint,
+                    (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Float64}, Int64, Int32, Float64, Int32, Int32),
+                    context(), d.handle, coef, n, order, beti(beam), nturns, turn), "tp_tpsa_ringpass")
+    end
+    coef, exps
+end
+
 end # module
