@@ -153,72 +153,59 @@ __device__ __forceinline__ TCtx* ctx_of(const Tv& a, const Tv& b) { return a.x ?
 
 __device__ __forceinline__ double cst(const Tv& a) { return a.p ? a.p[0] : a.c; }
 
-__device__ Tv operator+(const Tv& a, const Tv& b) {
-    if (!a.p && !b.p) return Tv(a.c + b.c);
-    TCtx* x = ctx_of(a, b);
-    ++x->nlin;
-    double* r = t_alloc(x);
-    const int M = x->M;
-    for (int k = threadIdx.x; k < M; k += blockDim.x) {
-        double v;
-        if (!a.p) v = k == 0 ? a.c + b.p[0] : b.p[k];
-        else if (!b.p) v = k == 0 ? a.p[0] + b.c : a.p[k];
-        else v = a.p[k] + b.p[k];
-        r[k] = v;
+// Elementwise kernels and the truncated product on plain restrict pointers:
+// the loops keep their pointers and sizes in registers (through the value
+// structs, every store could alias them and force reloads).
+static __device__ __forceinline__ void ew_add(double* __restrict__ r, const double* __restrict__ ap, double ac,
+                                              const double* __restrict__ bp, double bc, int M, bool sub) {
+    const int n = blockDim.x;
+    if (!ap) {
+        for (int k = threadIdx.x; k < M; k += n) r[k] = k == 0 ? (sub ? ac - bp[0] : ac + bp[0]) : (sub ? -bp[k] : bp[k]);
+    } else if (!bp) {
+        for (int k = threadIdx.x; k < M; k += n) r[k] = k == 0 ? (sub ? ap[0] - bc : ap[0] + bc) : ap[k];
+    } else if (sub) {
+        for (int k = threadIdx.x; k < M; k += n) r[k] = ap[k] - bp[k];
+    } else {
+        for (int k = threadIdx.x; k < M; k += n) r[k] = ap[k] + bp[k];
     }
     __syncthreads();
-    return Tv(r, x);
 }
 
-__device__ Tv operator-(const Tv& a) {
-    if (!a.p) return Tv(-a.c);
-    ++a.x->nlin;
-    double* r = t_alloc(a.x);
-    for (int k = threadIdx.x; k < a.x->M; k += blockDim.x) r[k] = -a.p[k];
+static __device__ __forceinline__ void ew_scale(double* __restrict__ r, const double* __restrict__ ap, double s,
+                                                int M) {
+    for (int k = threadIdx.x; k < M; k += blockDim.x) r[k] = ap[k] * s;
     __syncthreads();
-    return Tv(r, a.x);
 }
 
-__device__ Tv operator-(const Tv& a, const Tv& b) {
-    if (!a.p && !b.p) return Tv(a.c - b.c);
-    TCtx* x = ctx_of(a, b);
-    ++x->nlin;
-    double* r = t_alloc(x);
-    const int M = x->M;
+static __device__ __forceinline__ void ew_div(double* __restrict__ r, const double* __restrict__ ap, double s,
+                                              int M) {
+    for (int k = threadIdx.x; k < M; k += blockDim.x) r[k] = ap[k] / s;
+    __syncthreads();
+}
+
+static __device__ __forceinline__ void ew_neg(double* __restrict__ r, const double* __restrict__ ap, int M) {
+    for (int k = threadIdx.x; k < M; k += blockDim.x) r[k] = -ap[k];
+    __syncthreads();
+}
+
+static __device__ __forceinline__ void ew_copy(double* __restrict__ r, const double* __restrict__ ap, int M) {
+    for (int k = threadIdx.x; k < M; k += blockDim.x) r[k] = ap[k];
+    __syncthreads();
+}
+
+// Truncated product r = a * b over the pair table (r distinct from a and b);
+// four products in flight, summed in pair order (the oracle's order).
+static __device__ __noinline__ void t_mul_raw(double* __restrict__ r, const double* __restrict__ ap,
+                                              const double* __restrict__ bp, const int32_t* __restrict__ poff,
+                                              const uint32_t* __restrict__ pairs, int M) {
     for (int k = threadIdx.x; k < M; k += blockDim.x) {
-        double v;
-        if (!a.p) v = k == 0 ? a.c - b.p[0] : -b.p[k];
-        else if (!b.p) v = k == 0 ? a.p[0] - b.c : a.p[k];
-        else v = a.p[k] - b.p[k];
-        r[k] = v;
-    }
-    __syncthreads();
-    return Tv(r, x);
-}
-
-__device__ Tv t_scale(const Tv& a, double s) {
-    ++a.x->nlin;
-    double* r = t_alloc(a.x);
-    for (int k = threadIdx.x; k < a.x->M; k += blockDim.x) r[k] = a.p[k] * s;
-    __syncthreads();
-    return Tv(r, a.x);
-}
-
-// Truncated product into r (r distinct from a and b).
-__device__ void t_mul_into(double* r, const Tv& a, const Tv& b, TCtx* x) {
-    ++x->nmul;
-    const int M = x->M;
-    const double* ap = a.p;
-    const double* bp = b.p;
-    for (int k = threadIdx.x; k < M; k += blockDim.x) {
-        int p = x->poff[k];
-        const int p1 = x->poff[k + 1];
-        uint32_t q = x->pairs[p];
+        int p = poff[k];
+        const int p1 = poff[k + 1];
+        uint32_t q = pairs[p];
         double s = ap[q & 0xffffu] * bp[q >> 16];
         ++p;
-        // four products in flight, summed in pair order (the oracle's order)
         for (; p + 4 <= p1; p += 4) {
-            const uint32_t q0 = x->pairs[p], q1 = x->pairs[p + 1], q2 = x->pairs[p + 2], q3 = x->pairs[p + 3];
+            const uint32_t q0 = pairs[p], q1 = pairs[p + 1], q2 = pairs[p + 2], q3 = pairs[p + 3];
             const double m0 = ap[q0 & 0xffffu] * bp[q0 >> 16];
             const double m1 = ap[q1 & 0xffffu] * bp[q1 >> 16];
             const double m2 = ap[q2 & 0xffffu] * bp[q2 >> 16];
@@ -229,12 +216,50 @@ __device__ void t_mul_into(double* r, const Tv& a, const Tv& b, TCtx* x) {
             s = s + m3;
         }
         for (; p < p1; ++p) {
-            q = x->pairs[p];
+            q = pairs[p];
             s = s + ap[q & 0xffffu] * bp[q >> 16];
         }
         r[k] = s;
     }
     __syncthreads();
+}
+
+__device__ Tv operator+(const Tv& a, const Tv& b) {
+    if (!a.p && !b.p) return Tv(a.c + b.c);
+    TCtx* x = ctx_of(a, b);
+    ++x->nlin;
+    double* r = t_alloc(x);
+    ew_add(r, a.p, a.c, b.p, b.c, x->M, false);
+    return Tv(r, x);
+}
+
+__device__ Tv operator-(const Tv& a) {
+    if (!a.p) return Tv(-a.c);
+    ++a.x->nlin;
+    double* r = t_alloc(a.x);
+    ew_neg(r, a.p, a.x->M);
+    return Tv(r, a.x);
+}
+
+__device__ Tv operator-(const Tv& a, const Tv& b) {
+    if (!a.p && !b.p) return Tv(a.c - b.c);
+    TCtx* x = ctx_of(a, b);
+    ++x->nlin;
+    double* r = t_alloc(x);
+    ew_add(r, a.p, a.c, b.p, b.c, x->M, true);
+    return Tv(r, x);
+}
+
+__device__ Tv t_scale(const Tv& a, double s) {
+    ++a.x->nlin;
+    double* r = t_alloc(a.x);
+    ew_scale(r, a.p, s, a.x->M);
+    return Tv(r, a.x);
+}
+
+__device__ __forceinline__ void t_mul_into(double* r, const Tv& a, const Tv& b, TCtx* x) {
+    ++x->nmul;
+    t_mul_raw(r, a.p, b.p, x->poff, x->pairs, x->M);
 }
 
 __device__ Tv operator*(const Tv& a, const Tv& b) {
@@ -298,8 +323,12 @@ __device__ Tv t_apply(TFn f, const Tv& a) {
     double* s0 = t_alloc(x);
     double* s1 = t_alloc(x);
     double* ab = t_alloc(x);
-    for (int k = threadIdx.x; k < M; k += blockDim.x) ab[k] = k == 0 ? 0.0 : a.p[k];
-    __syncthreads();
+    {
+        const double* __restrict__ ap = a.p;
+        double* __restrict__ abr = ab;
+        for (int k = threadIdx.x; k < M; k += blockDim.x) abr[k] = k == 0 ? 0.0 : ap[k];
+        __syncthreads();
+    }
     // r = c_N (a number); r = r * abar -> c_N abar (a scaling); then r = r + c_k
     double* r = s0;
     double* t = s1;
@@ -308,22 +337,25 @@ __device__ Tv t_apply(TFn f, const Tv& a) {
         __syncthreads();
     } else {
         ++x->nlin;
-        for (int k = threadIdx.x; k < M; k += blockDim.x) {
-            const double v = ab[k] * c[N];
-            r[k] = k == 0 ? v + c[N - 1] : v;
+        {
+            const double cn = c[N], cn1 = c[N - 1];
+            const double* __restrict__ abr = ab;
+            double* __restrict__ rr = r;
+            for (int k = threadIdx.x; k < M; k += blockDim.x) {
+                const double v = abr[k] * cn;
+                rr[k] = k == 0 ? v + cn1 : v;
+            }
+            __syncthreads();
         }
-        __syncthreads();
         for (int j = N - 2; j >= 0; --j) {
-            t_mul_into(t, Tv(r, x), Tv(ab, x), x);
+            ++x->nmul;
+            t_mul_raw(t, r, ab, x->poff, x->pairs, M);
             if (threadIdx.x == 0) t[0] = t[0] + c[j];
             __syncthreads();
             double* sw = r; r = t; t = sw;
         }
     }
-    if (r != s0) {
-        for (int k = threadIdx.x; k < M; k += blockDim.x) s0[k] = r[k];
-        __syncthreads();
-    }
+    if (r != s0) ew_copy(s0, r, M);
     x->top = base + 1;
     return Tv(s0, x);
 }
@@ -340,8 +372,7 @@ __device__ Tv operator/(const Tv& a, const Tv& b) {
         if (!a.p) return Tv(a.c / b.c);
         ++a.x->nlin;
         double* r = t_alloc(a.x);
-        for (int k = threadIdx.x; k < a.x->M; k += blockDim.x) r[k] = a.p[k] / b.c;
-        __syncthreads();
+        ew_div(r, a.p, b.c, a.x->M);
         return Tv(r, a.x);
     }
     return a * inv(b);
@@ -354,8 +385,14 @@ struct TState {
     __device__ void set(int i, const Tv& v) {
         double* d = r[i].p;
         if (v.p == d) return;
-        for (int k = threadIdx.x; k < x->M; k += blockDim.x) d[k] = v.p ? v.p[k] : (k == 0 ? v.c : 0.0);
-        __syncthreads();
+        const int M = x->M;
+        if (v.p) {
+            ew_copy(d, v.p, M);
+        } else {
+            const double vc = v.c;
+            for (int k = threadIdx.x; k < M; k += blockDim.x) d[k] = k == 0 ? vc : 0.0;
+            __syncthreads();
+        }
     }
 };
 
@@ -367,10 +404,7 @@ __device__ Tv t_keep(const Tv& v, TCtx* x, int& mark) {
         return v;
     }
     double* d = x->pool + size_t(mark) * x->M;
-    if (v.p != d) {
-        for (int k = threadIdx.x; k < x->M; k += blockDim.x) d[k] = v.p[k];
-        __syncthreads();
-    }
+    if (v.p != d) ew_copy(d, v.p, x->M);
     x->top = ++mark;
     return Tv(d, x);
 }
@@ -678,11 +712,8 @@ __device__ void t_sgb(TState& S, const double* w) {
     // px, py accumulate in two work slots
     double* pxs = t_alloc(S.x);
     double* pys = t_alloc(S.x);
-    for (int k = threadIdx.x; k < S.x->M; k += blockDim.x) {
-        pxs[k] = r[1].p[k];
-        pys[k] = r[3].p[k];
-    }
-    __syncthreads();
+    ew_copy(pxs, r[1].p, S.x->M);
+    ew_copy(pys, r[3].p, S.x->M);
     Tv px(pxs, S.x), py(pys, S.x);
     const int m2 = S.x->top;
     for (int i = 0; i < nz; ++i) {
@@ -692,11 +723,8 @@ __device__ void t_sgb(TState& S, const double* w) {
         Tv g = KEEP(Tv(wt[i]) * exp(Tv(-0.5) * (dx * dx / sx2 + dy * dy / sy2)));
         Tv pxn = KEEP(px - factor * g * dx / sx2);
         Tv pyn = KEEP(py - factor * g * dy / sy2);
-        for (int k = threadIdx.x; k < S.x->M; k += blockDim.x) {
-            pxs[k] = pxn.p[k];
-            pys[k] = pyn.p[k];
-        }
-        __syncthreads();
+        ew_copy(pxs, pxn.p, S.x->M);
+        ew_copy(pys, pyn.p, S.x->M);
         S.x->top = m2;
     }
     S.set(1, px);
