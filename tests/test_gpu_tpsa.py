@@ -135,3 +135,23 @@ def test_work_statistics():
     assert st["maps"] == 3 and st["order"] == 3 and st["coefficients"] == 84
     assert st["series_mul"] > 0 and st["flops"] > 0 and st["kernel_ms"] > 0
     assert 6 < st["slots_used"] <= st["slots"]
+
+
+def test_core_kinds_fit_the_small_pool():
+    """Tables of the integrator core use the 18-series pool: drifts, multipoles
+    up to octupole, thin kicks of order 3, bends with all edge methods, RF."""
+    lat = tp.Lattice([
+        tp.Drift(0.3), tp.Quadrupole(0.4, 1.2), tp.Sextupole(0.2, 25.0), tp.Octupole(0.2, 300.0),
+        tp.ThinMultipole(0.0, [0.0, 0.01, 0.0, 0.5], [0.0, 0.1, 4.0, 30.0], max_order=3),
+        tp.SBend(0.9, 0.15, 0.03, 0.02, fint1=0.5, fint2=0.4, gap=0.05, fringe_bend_entrance=3, fringe_bend_exit=2,
+                 polynom_b=[0.0, -0.3, 1.5, 10.0], max_order=3),
+        tp.SBend(0.7, -0.08, 0.01, 0.0, fringe_bend_entrance=1, fringe_bend_exit=1),
+        tp.RFCavity(0.2, 2e6, 500e6, 0.002, philag=0.3, energy=E0),
+        tp.Drift(0.5),
+    ])
+    refs = _refs(3, 17)
+    for order in (2, 4):
+        dev = tp.tpsa.ringpass(lat, [tp.polyseries_variables(r, order) for r in refs], tp.Beam(E0), 2)
+        st = tp.tpsa.last_stats()
+        assert st["slots"] == 18 and st["slots_used"] <= 18
+        _assert_same(np.stack([m.coef for m in dev]), _oracle_maps(lat, refs, order, nturns=2))

@@ -7,7 +7,7 @@
 // One CTA tracks one map at a time (a persistent loop over the maps); its
 // threads share every series operation, each thread owning the coefficients
 // k = tid, tid + blockDim, ...; a __syncthreads() ends every operation.  The
-// series live in a pool of 28 or 40 slots of M doubles (40 when the lattice
+// series live in a pool of 18 or 40 slots of M doubles (40 when the lattice
 // holds the longer bodies: solenoid, corrector, rotations, beam-beam, crab and
 // accelerating cavities, misalignment rows), in shared memory when
 // it fits and in a per-CTA global slab otherwise.
@@ -50,7 +50,7 @@ namespace {
 using namespace tp::dev;
 
 constexpr int kTpsaMaxOrder = 10;
-constexpr int kSlotsCore = 28;        // series per map for drifts, kicks, bends, RF (25 measured at most)
+constexpr int kSlotsCore = 18;        // series per map for drifts, kicks, bends, RF
 constexpr int kSlotsRare = 40;        // with the longer bodies (solenoid, corrector, rotations, beam-beam)
 constexpr int kTpsaScratchTable = 13; // context scratch slots used here
 constexpr int kTpsaScratchMaps = 14;
@@ -416,16 +416,18 @@ __device__ Tv t_keep(const Tv& v, TCtx* x, int& mark) {
 // drift6_tpsa (:57-65), L / sqrt(pz2) as L * pz2^(-1/2)
 __device__ void t_drift(TState& S, double L, double beti) {
     const int m = S.x->top;
+    int mk = m;
     Tv* r = S.r;
     {
-        Tv pz2 = Tv(1.0) + Tv(2.0) * r[5] * Tv(beti) + r[5] * r[5] - r[1] * r[1] - r[3] * r[3];
-        Tv NormL = Tv(L) * rsqrt(pz2);
-        Tv x_new = r[0] + NormL * r[1];
-        Tv y_new = r[2] + NormL * r[3];
-        Tv z_new = r[4] + NormL * (Tv(beti) + r[5]) - Tv(L) * Tv(beti);
-        S.set(0, x_new);
-        S.set(2, y_new);
-        S.set(4, z_new);
+        Tv pz2 = KEEP(Tv(1.0) + Tv(2.0) * r[5] * Tv(beti) + r[5] * r[5] - r[1] * r[1] - r[3] * r[3]);
+        Tv NormL = KEEP(Tv(L) * rsqrt(pz2));
+        // x, y and z do not feed each other: each is stored as soon as it is known
+        const int m2 = S.x->top;
+        S.set(0, r[0] + NormL * r[1]);
+        S.x->top = m2;
+        S.set(2, r[2] + NormL * r[3]);
+        S.x->top = m2;
+        S.set(4, r[4] + NormL * (Tv(beti) + r[5]) - Tv(L) * Tv(beti));
     }
     S.x->top = m;
 }
@@ -434,26 +436,38 @@ __device__ void t_drift(TState& S, double L, double beti) {
 __device__ void t_kick(TState& S, const double* pa, const double* pb, double L, int mo, bool bend, double irho,
                        double beti) {
     const int m = S.x->top;
-    int mk = m;
     Tv* r = S.r;
     Tv ReSum(pb[mo]), ImSum(pa[mo]);
-    for (int i = mo - 1; i >= 0; --i) {
-        Tv ReSumTemp = KEEP(ReSum * r[0] - ImSum * r[2] + Tv(pb[i]));
-        ImSum = KEEP(ImSum * r[0] + ReSum * r[2] + Tv(pa[i]));
-        ReSum = ReSumTemp;
+    // the running sums live in slots m and m+1 whatever the order
+    if (m + 2 > S.x->nslots) {
+        if (threadIdx.x == 0) atomicOr(S.x->err, TE_SLOTS);
+        return;
     }
+    double* const re_slot = S.x->pool + size_t(m) * S.x->M;
+    double* const im_slot = re_slot + S.x->M;
+    for (int i = mo - 1; i >= 0; --i) {
+        int mk = m + 2;
+        S.x->top = mk;
+        Tv ReSumTemp = KEEP(ReSum * r[0] - ImSum * r[2] + Tv(pb[i]));
+        Tv ImSumNew = KEEP(ImSum * r[0] + ReSum * r[2] + Tv(pa[i]));
+        ew_copy(re_slot, ReSumTemp.p, S.x->M);
+        ew_copy(im_slot, ImSumNew.p, S.x->M);
+        ReSum = Tv(re_slot, S.x);
+        ImSum = Tv(im_slot, S.x);
+    }
+    const int m2 = mo > 0 ? m + 2 : m;
+    S.x->top = m2;
+    // px, py and z do not feed each other: each is stored as soon as it is known
     if (!bend) {
-        Tv px_new = r[1] - Tv(L) * ReSum;
-        Tv py_new = r[3] + Tv(L) * ImSum;
-        S.set(1, px_new);
-        S.set(3, py_new);
+        S.set(1, r[1] - Tv(L) * ReSum);
+        S.x->top = m2;
+        S.set(3, r[3] + Tv(L) * ImSum);
     } else {
-        Tv px_new = r[1] - Tv(L) * (ReSum - (r[5] - r[0] * Tv(irho)) * Tv(irho));
-        Tv py_new = r[3] + Tv(L) * ImSum;
-        Tv z_new = r[4] + Tv(L) * Tv(irho) * r[0] * Tv(beti);
-        S.set(1, px_new);
-        S.set(3, py_new);
-        S.set(4, z_new);
+        S.set(1, r[1] - Tv(L) * (ReSum - (r[5] - r[0] * Tv(irho)) * Tv(irho)));
+        S.x->top = m2;
+        S.set(3, r[3] + Tv(L) * ImSum);
+        S.x->top = m2;
+        S.set(4, r[4] + Tv(L) * Tv(irho) * r[0] * Tv(beti));
     }
     S.x->top = m;
 }
@@ -969,7 +983,9 @@ TP_API int tp_tpsa_ringpass(tp_ctx* ctx, const tp_lattice* lat, double* maps, in
     TPSA_CUDA(cudaMemcpyAsync(d_maps, maps, map_bytes, cudaMemcpyHostToDevice, s));
 
     // launch shape: threads ~ M/2 (32..256); pool in shared memory when it fits
-    int block = (M / 2 + 31) / 32 * 32;
+    // about four coefficients per thread: enough work per operation to carry
+    // its barrier, and small CTAs so that registers allow 8 maps per SM
+    int block = (M / 4 + 31) / 32 * 32;
     block = std::max(32, std::min(256, block));
     // series slots: the longer bodies hold more work series at once
     bool rare = L.nmis > 0;
