@@ -60,6 +60,8 @@ def parse():
     p.add_argument("--turns", type=int, default=0, help="turns per step (0: the workload's default)")
     p.add_argument("--nvar", type=int, default=0, help="variants of the batched workloads (0: default)")
     p.add_argument("--contract", action="store_true", help="kernels built with FMA contraction")
+    p.add_argument("--table-smem", action="store_true",
+                   help="stage element tables into shared memory (default: read through the L1 cache)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-adjoint", action="store_true", help="default workload: skip the adjoint ratio")
@@ -356,7 +358,8 @@ def main_track(args, tp, torch, rank, world, local, dist):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox Gaussian beam + DA grid)",
             "config": {"workload": w["name"], "turns_per_step": turns, "particles_per_gpu": n,
                        "elements": len(lat), "l2": "flushed between timed steps (256 MiB write)",
-                       "fp": "FMA contraction" if args.contract else "no FMA contraction (reference operation order)"},
+                       "fp": "FMA contraction" if args.contract else "no FMA contraction (reference operation order)",
+                       "element_table": "shared memory (TMA bulk copy)" if args.table_smem else "L1 cache"},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": DRAM_BYTES_PER_PARTICLE * n,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on "
@@ -654,6 +657,7 @@ def main():
     import torch
     import __graft_entry__
     tp = __graft_entry__.load_package()
+    tp.tracking.TABLE_IN_SMEM = bool(args.table_smem)
     torch.cuda.set_device(local)
     dist = None
     if world > 1:

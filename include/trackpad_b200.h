@@ -187,7 +187,12 @@ typedef struct tp_opts {
                                   calls the faster (all give identical results);
                                   1 = static, 2 = lane refill (batched: lanes of a
                                   variant refill from that variant's particles)   */
-    int32_t reserved0;
+    int32_t table_in_smem;     /* 1: stage the element table into shared memory by a
+                                  bulk (TMA) copy at the start of each block; default
+                                  0: read it through the L1 cache.  On the DBA ring the
+                                  staged table (37.5 KB per block) leaves the L1 too
+                                  small for the kernels' stack, and staging measured
+                                  5 % slower                                       */
     double aperture_x;         /* rectangular aperture half widths [m]; a value   */
     double aperture_y;         /* <= 0 disables it (reference limits remain)      */
     void* stream;              /* cudaStream_t to run on; NULL = context stream   */

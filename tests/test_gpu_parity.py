@@ -373,3 +373,25 @@ def test_unsupported_schedule_outside_range():
                                    np.zeros(10, np.int64).ctypes.data_as(C.c_void_p), None, None,
                                    C.c_double(1.0001), 5, C.c_double(0), C.c_double(0), 0, C.byref(o))
     assert st == tp._abi.TP_ERANGE
+
+
+def test_table_in_shared_memory_or_l1_gives_the_same_bits():
+    """tp_opts.table_in_smem only moves the element table (shared memory by a
+    bulk copy, or the L1 cache): tracking and gradients are bit-identical."""
+    lat, beam = W.dba_ring(cells=2), W.dba_beam()
+    c0 = W.gaussian(4096, seed=5)
+    params = W.magnet_indices(lat)
+    out = []
+    for flag in (False, True):
+        tp.tracking.TABLE_IN_SMEM = flag
+        try:
+            c = np.asfortranarray(c0.copy())
+            lost = np.zeros(len(c), np.int64)
+            tp.ringpass_(c, lat, beam, lost, 5, aperture=0.02)
+            loss, g = tp.ringpass_adjoint(c0, lat, beam, None, 3, params, sigma=1e-4, aperture=0.02)[:2]
+            out.append((c, lost, loss, g))
+        finally:
+            tp.tracking.TABLE_IN_SMEM = False
+    (c1, l1, s1, g1), (c2, l2, s2, g2) = out
+    assert np.array_equal(c1, c2, equal_nan=True) and np.array_equal(l1, l2)
+    assert s1 == s2 and np.array_equal(g1, g2)

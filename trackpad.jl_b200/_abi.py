@@ -63,7 +63,7 @@ class TpOpts(C.Structure):
     _fields_ = [
         ("size", C.c_int32), ("exact_hamiltonian", C.c_int32), ("device_pointers", C.c_int32),
         ("fp_contract", C.c_int32), ("block_size", C.c_int32), ("ppt", C.c_int32), ("schedule", C.c_int32),
-        ("reserved0", C.c_int32), ("aperture_x", C.c_double), ("aperture_y", C.c_double), ("stream", C.c_void_p),
+        ("table_in_smem", C.c_int32), ("aperture_x", C.c_double), ("aperture_y", C.c_double), ("stream", C.c_void_p),
     ]
 
 

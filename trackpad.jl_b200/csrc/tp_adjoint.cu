@@ -585,7 +585,7 @@ int run_adjoint(tp_ctx* c, const std::vector<const tp_lattice*>& lats, const std
                 int32_t turn0, const int32_t* params, const std::vector<int32_t>& poff_params, int mode,
                 double sigma, double lost_weight, int32_t K, double limx, double limy, bool exact, cudaStream_t s,
                 double* h_loss, double* h_grad, double* d_fin_out, int64_t* d_lost_out, double* d_seed_out,
-                int64_t* h_surv, float* ms_fwd, float* ms_rev, double* rec_err, double* units) {
+                int64_t* h_surv, float* ms_fwd, float* ms_rev, double* rec_err, double* units, bool table_smem) {
     HostPlan P;
     int st = make_plan(lats, npart, betis, params, poff_params, turn0, nturns, &P);
     if (st != TP_OK) return st;
@@ -662,7 +662,7 @@ int run_adjoint(tp_ctx* c, const std::vector<const tp_lattice*>& lats, const std
     const size_t smem_bytes = (P.table.size() + info_words) * 8;
     a.smem_words = 0;
     size_t smem = 0;
-    if (nvar == 1 && smem_bytes + 1024 <= ch.smem_optin) {
+    if (table_smem && nvar == 1 && smem_bytes + 1024 <= ch.smem_optin) {
         a.smem_words = int32_t(P.table.size() + info_words);
         smem = smem_bytes;
     }
@@ -840,7 +840,7 @@ TP_API int tp_ringpass_adjoint(tp_ctx* ctx, const tp_lattice* lat, const double*
     st = run_adjoint(ctx, lats, {n}, {beti}, d_c, d_l, nturns, turn0, param_elems, poff, 0, loss->sigma,
                      loss->lost_weight, checkpoint_every, limit_of(o.aperture_x), limit_of(o.aperture_y),
                      o.exact_hamiltonian != 0, s, loss_out, grad.data(), d_fin, d_lost, nullptr, &surv, &msf, &msr,
-                     &rec, &units);
+                     &rec, &units, o.table_in_smem != 0);
     if (st != TP_OK) return st;
     if (nparams > 0) std::memcpy(grad_out, grad.data(), size_t(nparams) * 8);
     if (!dev && (coords_out || lost_out)) {
@@ -923,7 +923,7 @@ TP_API int tp_ringpass_adjoint_batched(tp_ctx* ctx, tp_batch* b, const double* c
     st = run_adjoint(ctx, lats, np, bt, d_c, d_l, nturns, turn0, param_elems, pofs, 0, loss->sigma,
                      loss->lost_weight, checkpoint_every, limit_of(o.aperture_x), limit_of(o.aperture_y),
                      o.exact_hamiltonian != 0, s, loss_out, grad.data(), nullptr, nullptr, nullptr, surv.data(), &msf,
-                     &msr, &rec, &units);
+                     &msr, &rec, &units, o.table_in_smem != 0);
     if (st != TP_OK) return st;
     if (pofs[size_t(nvar)] > 0) std::memcpy(grad_out, grad.data(), size_t(pofs[size_t(nvar)]) * 8);
     tp_stats& S = *ctx_stats(ctx);
@@ -984,7 +984,7 @@ TP_API int tp_one_turn_jacobian(tp_ctx* ctx, const tp_lattice* lat, const double
     // K = 1: the reverse sweep rebuilds one turn at a time.
     st = run_adjoint(ctx, lats, {n6}, {beti}, static_cast<const double*>(d_rep), nullptr, nturns, turn0, nullptr, poff,
                      1, 1.0, 0.0, 1, 1.0, 1.0, o.exact_hamiltonian != 0, s, nullptr, nullptr, nullptr, nullptr,
-                     static_cast<double*>(d_seed), &surv, &msf, &msr, &rec, &units);
+                     static_cast<double*>(d_seed), &surv, &msf, &msr, &rec, &units, o.table_in_smem != 0);
     if (st != TP_OK) return st;
     // run_adjoint left the flags in its own scratch slot
     void* d_lost;

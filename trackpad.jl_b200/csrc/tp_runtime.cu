@@ -722,7 +722,7 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     a.err = c->err;
     a.nvar = 0;
     const size_t table_bytes = L->program.size() * sizeof(double);
-    const size_t smem = table_bytes + 64 <= c->smem_optin ? table_bytes : 0;
+    const size_t smem = o.table_in_smem && table_bytes + 64 <= c->smem_optin ? table_bytes : 0;
     a.smem_words = smem ? int32_t(L->program.size()) : 0;
     // Launch configuration: static for single passes; for multi-turn tracks the
     // schedule the caller asks for, else the tuned one (lane refill frees the

@@ -275,8 +275,14 @@ def spos(lat, time=0.0, turn=0):
 # ---------------------------------------------------------------------------
 # Tracking calls
 # ---------------------------------------------------------------------------
+# Stage element tables into shared memory (tp_opts.table_in_smem); off by
+# default, where the tables are read through the L1 cache.
+TABLE_IN_SMEM = False
+
+
 def _opts(aperture, exact, contract, device, block_size=0, schedule=0, stream=None):
     o = _abi.TpOpts()
+    o.table_in_smem = 1 if TABLE_IN_SMEM else 0
     o.size = C.sizeof(_abi.TpOpts)
     o.exact_hamiltonian = 1 if exact else 0
     o.device_pointers = 1 if device else 0
