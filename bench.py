@@ -42,7 +42,7 @@ LOST_WEIGHT = 1e3
 # DRAM bytes per particle of one tracking launch: ncu capture of track_single on
 # the DBA ring, 69,632 particles x 10 turns (5.425 MB read + written).  Traffic
 # grows with the particle count (the table lives in shared memory).
-DRAM_BYTES_PER_PARTICLE = 5.425152e6 / 69632
+DRAM_BYTES_PER_PARTICLE = 4.645888e6 / 69632
 
 
 def parse():
