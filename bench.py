@@ -42,7 +42,7 @@ LOST_WEIGHT = 1e3
 # DRAM bytes per particle of one tracking launch: ncu capture of track_single on
 # the DBA ring, 69,632 particles x 10 turns (5.425 MB read + written).  Traffic
 # grows with the particle count (the table lives in shared memory).
-DRAM_BYTES_PER_PARTICLE = 4.645888e6 / 69632
+DRAM_BYTES_PER_PARTICLE = 1.407376e9 / 135168
 
 
 def parse():
@@ -363,7 +363,8 @@ def main_track(args, tp, torch, rank, world, local, dist):
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                          "frac": achieved / peak, "traffic": DRAM_BYTES_PER_PARTICLE * n,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on "
-                                           "69,632 particles x 10 turns, scaled by particles",
+                                           "135,168 particles x 10 turns (one full wave), scaled by particles; "
+                                           "almost all of it is the write-back of spilled stack lines",
                          "peak_source": "measured FP64 FMA throughput of this device (tp_probe_fp64_peak)",
                          "flops_per_launch": flops / args.steps, "kernel_ms": k_ms},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
