@@ -195,9 +195,12 @@ static __device__ __forceinline__ void ew_copy(double* __restrict__ r, const dou
 
 // Truncated product r = a * b over the pair table (r distinct from a and b);
 // four products in flight, summed in pair order (the oracle's order).
+// With addc, the constant c is then added to the constant part (Horner's
+// "+ c_k"), in the same pass.
 static __device__ __noinline__ void t_mul_raw(double* __restrict__ r, const double* __restrict__ ap,
                                               const double* __restrict__ bp, const int32_t* __restrict__ poff,
-                                              const uint32_t* __restrict__ pairs, int M) {
+                                              const uint32_t* __restrict__ pairs, int M, bool addc = false,
+                                              double c = 0.0) {
     for (int k = threadIdx.x; k < M; k += blockDim.x) {
         int p = poff[k];
         const int p1 = poff[k + 1];
@@ -219,7 +222,7 @@ static __device__ __noinline__ void t_mul_raw(double* __restrict__ r, const doub
             q = pairs[p];
             s = s + ap[q & 0xffffu] * bp[q >> 16];
         }
-        r[k] = s;
+        r[k] = (addc && k == 0) ? s + c : s;
     }
     __syncthreads();
 }
@@ -255,6 +258,45 @@ __device__ Tv t_scale(const Tv& a, double s) {
     double* r = t_alloc(a.x);
     ew_scale(r, a.p, s, a.x->M);
     return Tv(r, a.x);
+}
+
+// dst = add + a*b (sub: add - a*b) with the product summed as in t_mul_raw and
+// then combined, the rounding of the two separate operations; add may be dst.
+static __device__ __noinline__ void t_mul_acc_raw(double* dst, const double* add, const double* __restrict__ ap,
+                                                  const double* __restrict__ bp, const int32_t* __restrict__ poff,
+                                                  const uint32_t* __restrict__ pairs, int M, bool sub) {
+    for (int k = threadIdx.x; k < M; k += blockDim.x) {
+        int p = poff[k];
+        const int p1 = poff[k + 1];
+        uint32_t q = pairs[p];
+        double s = ap[q & 0xffffu] * bp[q >> 16];
+        ++p;
+        for (; p + 4 <= p1; p += 4) {
+            const uint32_t q0 = pairs[p], q1 = pairs[p + 1], q2 = pairs[p + 2], q3 = pairs[p + 3];
+            const double m0 = ap[q0 & 0xffffu] * bp[q0 >> 16];
+            const double m1 = ap[q1 & 0xffffu] * bp[q1 >> 16];
+            const double m2 = ap[q2 & 0xffffu] * bp[q2 >> 16];
+            const double m3 = ap[q3 & 0xffffu] * bp[q3 >> 16];
+            s = s + m0;
+            s = s + m1;
+            s = s + m2;
+            s = s + m3;
+        }
+        for (; p < p1; ++p) {
+            q = pairs[p];
+            s = s + ap[q & 0xffffu] * bp[q >> 16];
+        }
+        const double v = add[k];
+        dst[k] = sub ? v - s : v + s;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ void t_mul_acc(double* dst, const double* add, const Tv& a, const Tv& b, TCtx* x,
+                                          bool sub) {
+    ++x->nmul;
+    ++x->nlin;
+    t_mul_acc_raw(dst, add, a.p, b.p, x->poff, x->pairs, x->M, sub);
 }
 
 __device__ __forceinline__ void t_mul_into(double* r, const Tv& a, const Tv& b, TCtx* x) {
@@ -349,9 +391,7 @@ __device__ Tv t_apply(TFn f, const Tv& a) {
         }
         for (int j = N - 2; j >= 0; --j) {
             ++x->nmul;
-            t_mul_raw(t, r, ab, x->poff, x->pairs, M);
-            if (threadIdx.x == 0) t[0] = t[0] + c[j];
-            __syncthreads();
+            t_mul_raw(t, r, ab, x->poff, x->pairs, M, true, c[j]);
             double* sw = r; r = t; t = sw;
         }
     }
@@ -414,27 +454,84 @@ __device__ Tv t_keep(const Tv& v, TCtx* x, int& mark) {
 // Element maps (ext/TrackPadPolySeriesExt.jl).  Each releases its work slots.
 // ---------------------------------------------------------------------------
 // drift6_tpsa (:57-65), L / sqrt(pz2) as L * pz2^(-1/2)
+// Each statement is the reference's expression, evaluated with every sum of a
+// product fused into the product's pass (t_mul_acc): the same roundings in the
+// same order, fewer passes and barriers.
 __device__ void t_drift(TState& S, double L, double beti) {
-    const int m = S.x->top;
-    int mk = m;
+    TCtx* x = S.x;
+    const int m = x->top;
+    const int M = x->M;
     Tv* r = S.r;
+    // pz2 = 1 + 2 delta beti + delta^2 - px^2 - py^2, left to right
+    double* pz2 = t_alloc(x);
     {
-        Tv pz2 = KEEP(Tv(1.0) + Tv(2.0) * r[5] * Tv(beti) + r[5] * r[5] - r[1] * r[1] - r[3] * r[3]);
-        Tv NormL = KEEP(Tv(L) * rsqrt(pz2));
-        // x, y and z do not feed each other: each is stored as soon as it is known
-        const int m2 = S.x->top;
-        S.set(0, r[0] + NormL * r[1]);
-        S.x->top = m2;
-        S.set(2, r[2] + NormL * r[3]);
-        S.x->top = m2;
-        S.set(4, r[4] + NormL * (Tv(beti) + r[5]) - Tv(L) * Tv(beti));
+        const double* __restrict__ d = r[5].p;
+        for (int k = threadIdx.x; k < M; k += blockDim.x) {
+            const double v = (d[k] * 2.0) * beti;
+            pz2[k] = k == 0 ? 1.0 + v : v;
+        }
+        ++x->nlin;
+        __syncthreads();
     }
-    S.x->top = m;
+    t_mul_acc(pz2, pz2, r[5], r[5], x, false);
+    t_mul_acc(pz2, pz2, r[1], r[1], x, true);
+    t_mul_acc(pz2, pz2, r[3], r[3], x, true);
+    // NormL = L / sqrt(pz2) as L * pz2^(-1/2)
+    Tv NormL = t_scale(rsqrt(Tv(pz2, x)), L);
+    // x and y in place: x_k = x_k + (NormL px)_k
+    t_mul_acc(r[0].p, r[0].p, NormL, r[1], x, false);
+    t_mul_acc(r[2].p, r[2].p, NormL, r[3], x, false);
+    // z = z + NormL (beti + delta) - L beti
+    double* u = t_alloc(x);
+    {
+        const double* __restrict__ d = r[5].p;
+        for (int k = threadIdx.x; k < M; k += blockDim.x) u[k] = k == 0 ? beti + d[0] : d[k];
+        ++x->nlin;
+        __syncthreads();
+    }
+    t_mul_acc(r[4].p, r[4].p, NormL, Tv(u, x), x, false);
+    if (threadIdx.x == 0) r[4].p[0] = r[4].p[0] - L * beti;
+    __syncthreads();
+    x->top = m;
 }
 
 // strthinkick_tpsa (:78-92) and bndthinkick_tpsa (:94-112)
 __device__ void t_kick(TState& S, const double* pa, const double* pb, double L, int mo, bool bend, double irho,
                        double beti) {
+    if (mo == 1) {
+        // Order 1 (quadrupoles, dipole kicks): every output is a linear function
+        // of the coordinates, evaluated in one pass with the reference's
+        // operations per coefficient (the number terms only on the constant part).
+        TCtx* x = S.x;
+        const int M = x->M;
+        const double re1 = pb[1], im1 = pa[1], pb0 = pb[0], pa0 = pa[0];
+        const double Lirho = L * irho;
+        const double* __restrict__ xs = S.r[0].p;
+        const double* __restrict__ ys = S.r[2].p;
+        const double* __restrict__ ds = S.r[5].p;
+        double* pxs = S.r[1].p;
+        double* pys = S.r[3].p;
+        double* zs = S.r[4].p;
+        for (int k = threadIdx.x; k < M; k += blockDim.x) {
+            // ReSum = pb1 x - pa1 y + pb0, ImSum = pa1 x + pb1 y + pa0
+            double re = xs[k] * re1 - ys[k] * im1;
+            double im = xs[k] * im1 + ys[k] * re1;
+            if (k == 0) {
+                re = re + pb0;
+                im = im + pa0;
+            }
+            if (!bend) {
+                pxs[k] = pxs[k] - re * L;
+            } else {
+                pxs[k] = pxs[k] - (re - (ds[k] - xs[k] * irho) * irho) * L;
+                zs[k] = zs[k] + (xs[k] * Lirho) * beti;
+            }
+            pys[k] = pys[k] + im * L;
+        }
+        x->nlin += bend ? 3 : 2;
+        __syncthreads();
+        return;
+    }
     const int m = S.x->top;
     Tv* r = S.r;
     Tv ReSum(pb[mo]), ImSum(pa[mo]);
