@@ -60,7 +60,8 @@ def _assert_same(dev, ref):
         raise AssertionError(f"series differ: max |dev - ref| = {err:.3e} (max |ref| = {scale:.3e})")
 
 
-@pytest.mark.parametrize("order", [1, 2, 4])
+# order 5 is the first whose products are dealt to threads by pair count
+@pytest.mark.parametrize("order", [1, 2, 4, 5])
 def test_every_kind_matches_oracle_bitwise(order):
     lat = all_kinds_lattice()
     refs = _refs(5, 3)

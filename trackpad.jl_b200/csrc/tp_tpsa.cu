@@ -52,6 +52,11 @@ using namespace tp::dev;
 constexpr int kTpsaMaxOrder = 10;
 constexpr int kSlotsCore = 18;        // series per map for drifts, kicks, bends, RF
 constexpr int kSlotsRare = 40;        // with the longer bodies (solenoid, corrector, rotations, beam-beam)
+// busiest-thread pair count of the strided split above which product outputs
+// are dealt to threads by pair count instead
+#ifndef TP_TPSA_DEAL_MIN
+#define TP_TPSA_DEAL_MIN 64
+#endif
 constexpr int kTpsaScratchTable = 13; // context scratch slots used here
 constexpr int kTpsaScratchMaps = 14;
 constexpr int kTpsaScratchPool = 15;
@@ -120,8 +125,9 @@ const TpsaTables& tables_of(int N) {
 // ---------------------------------------------------------------------------
 struct TCtx {
     double* pool;            // nslots x M
-    const int32_t* poff;
+    const int4* otab;        // product output slots: {output k (-1: none), first pair, end pair, 0}
     const uint32_t* pairs;
+    int olen;                // product output slots (M, or more when dealt by pair count)
     int M, N, top, maxtop, nslots;
     int* err;                // TE_* bits
     unsigned long long nmul, nlin;  // series products and elementwise operations of this map
@@ -198,12 +204,15 @@ static __device__ __forceinline__ void ew_copy(double* __restrict__ r, const dou
 // With addc, the constant c is then added to the constant part (Horner's
 // "+ c_k"), in the same pass.
 static __device__ __noinline__ void t_mul_raw(double* __restrict__ r, const double* __restrict__ ap,
-                                              const double* __restrict__ bp, const int32_t* __restrict__ poff,
-                                              const uint32_t* __restrict__ pairs, int M, bool addc = false,
+                                              const double* __restrict__ bp, const int4* __restrict__ otab,
+                                              const uint32_t* __restrict__ pairs, int olen, bool addc = false,
                                               double c = 0.0) {
-    for (int k = threadIdx.x; k < M; k += blockDim.x) {
-        int p = poff[k];
-        const int p1 = poff[k + 1];
+    for (int o = threadIdx.x; o < olen; o += blockDim.x) {
+        const int4 e = otab[o];
+        const int k = e.x;
+        if (k < 0) continue;
+        int p = e.y;
+        const int p1 = e.z;
         uint32_t q = pairs[p];
         double s = ap[q & 0xffffu] * bp[q >> 16];
         ++p;
@@ -263,11 +272,14 @@ __device__ Tv t_scale(const Tv& a, double s) {
 // dst = add + a*b (sub: add - a*b) with the product summed as in t_mul_raw and
 // then combined, the rounding of the two separate operations; add may be dst.
 static __device__ __noinline__ void t_mul_acc_raw(double* dst, const double* add, const double* __restrict__ ap,
-                                                  const double* __restrict__ bp, const int32_t* __restrict__ poff,
-                                                  const uint32_t* __restrict__ pairs, int M, bool sub) {
-    for (int k = threadIdx.x; k < M; k += blockDim.x) {
-        int p = poff[k];
-        const int p1 = poff[k + 1];
+                                                  const double* __restrict__ bp, const int4* __restrict__ otab,
+                                                  const uint32_t* __restrict__ pairs, int olen, bool sub) {
+    for (int o = threadIdx.x; o < olen; o += blockDim.x) {
+        const int4 e = otab[o];
+        const int k = e.x;
+        if (k < 0) continue;
+        int p = e.y;
+        const int p1 = e.z;
         uint32_t q = pairs[p];
         double s = ap[q & 0xffffu] * bp[q >> 16];
         ++p;
@@ -296,12 +308,12 @@ __device__ __forceinline__ void t_mul_acc(double* dst, const double* add, const 
                                           bool sub) {
     ++x->nmul;
     ++x->nlin;
-    t_mul_acc_raw(dst, add, a.p, b.p, x->poff, x->pairs, x->M, sub);
+    t_mul_acc_raw(dst, add, a.p, b.p, x->otab, x->pairs, x->olen, sub);
 }
 
 __device__ __forceinline__ void t_mul_into(double* r, const Tv& a, const Tv& b, TCtx* x) {
     ++x->nmul;
-    t_mul_raw(r, a.p, b.p, x->poff, x->pairs, x->M);
+    t_mul_raw(r, a.p, b.p, x->otab, x->pairs, x->olen);
 }
 
 __device__ Tv operator*(const Tv& a, const Tv& b) {
@@ -391,7 +403,7 @@ __device__ Tv t_apply(TFn f, const Tv& a) {
         }
         for (int j = N - 2; j >= 0; --j) {
             ++x->nmul;
-            t_mul_raw(t, r, ab, x->poff, x->pairs, M, true, c[j]);
+            t_mul_raw(t, r, ab, x->otab, x->pairs, x->olen, true, c[j]);
             double* sw = r; r = t; t = sw;
         }
     }
@@ -909,8 +921,9 @@ struct TArgs {
     int32_t sched_stride, sched_turn0, sched_nturns;
     const double* sched;
     const MisalignDev* mis;
-    const int32_t* poff;
+    const int4* otab;
     const uint32_t* pairs;
+    int32_t olen;
     double* maps;            // nmaps x 6 x M
     int64_t nmaps;
     double* gpool;           // per-CTA slabs when the pool is not in shared memory
@@ -926,7 +939,8 @@ __global__ void __launch_bounds__(256) tpsa_track(TArgs a) {
     TCtx X;
     X.pool = a.gpool ? a.gpool + size_t(blockIdx.x) * a.slots * a.M : tsm;
     X.nslots = a.slots;
-    X.poff = a.poff;
+    X.otab = a.otab;
+    X.olen = a.olen;
     X.pairs = a.pairs;
     X.M = a.M;
     X.N = a.N;
@@ -1053,23 +1067,81 @@ TP_API int tp_tpsa_ringpass(tp_ctx* ctx, const tp_lattice* lat, double* maps, in
         std::memcpy(o.r1, m.r1, sizeof o.r1); std::memcpy(o.r2, m.r2, sizeof o.r2);
         for (int k = 0; k < 36; ++k) { o.r1nz |= m.r1[k] != 0.0; o.r2nz |= m.r2[k] != 0.0; }
     }
+    // launch shape: about four coefficients per thread, enough work per
+    // operation to carry its barrier, and small CTAs so that registers allow
+    // 8 maps per SM
+    int block = (M / 4 + 31) / 32 * 32;
+    block = std::max(32, std::min(256, block));
+    // Product outputs dealt to threads by pair count, longest first to the
+    // least loaded thread: a product takes as long as its busiest thread (at
+    // order 6 the strided split gave one thread 122 pairs, this one 76).  The
+    // sum of each output keeps its pair order, so the bits do not change.
+    // Measured on the FODO ring (six variables): orders 5 / 6 / 7 run 16 / 7 /
+    // 18 % faster; at orders 2 and 4, whose busiest thread sums 4 and 38 pairs,
+    // the indirection cost more than the balance saved (15 and 5 % slower), so
+    // the dealt order is used only when the strided split leaves a thread
+    // TP_TPSA_DEAL_MIN pairs or more and the dealt one lowers that.  Slot o of
+    // the table holds {output k (-1: none), first pair, end pair, 0}; thread t
+    // takes slots t, t + block, ...
+    std::vector<int32_t> otab;
+    {
+        auto npairs = [&](int32_t k) { return int64_t(T.poff[size_t(k) + 1]) - T.poff[size_t(k)]; };
+        int64_t strided_max = 0;
+        for (int t = 0; t < block; ++t) {
+            int64_t l = 0;
+            for (int k = t; k < M; k += block) l += npairs(k);
+            strided_max = std::max(strided_max, l);
+        }
+        std::vector<int32_t> idx(static_cast<size_t>(M));
+        for (int k = 0; k < M; ++k) idx[size_t(k)] = k;
+        std::stable_sort(idx.begin(), idx.end(), [&](int32_t u, int32_t v) {
+            return npairs(u) > npairs(v);
+        });
+        std::vector<int64_t> load(static_cast<size_t>(block), 0);
+        std::vector<std::vector<int32_t>> lists(static_cast<size_t>(block));
+        for (int32_t k : idx) {
+            size_t best = 0;
+            for (size_t t = 1; t < load.size(); ++t)
+                if (load[t] < load[best]) best = t;
+            load[best] += npairs(k);
+            lists[best].push_back(k);
+        }
+        const int64_t dealt_max = *std::max_element(load.begin(), load.end());
+        auto put = [&](size_t o, int32_t k) {
+            otab[4 * o] = k;
+            otab[4 * o + 1] = T.poff[size_t(k)];
+            otab[4 * o + 2] = T.poff[size_t(k) + 1];
+        };
+        if (strided_max >= TP_TPSA_DEAL_MIN && dealt_max < strided_max) {
+            size_t depth = 0;
+            for (const auto& l : lists) depth = std::max(depth, l.size());
+            otab.assign(4 * depth * size_t(block), 0);
+            for (size_t o = 0; o < depth * size_t(block); ++o) otab[4 * o] = -1;
+            for (size_t t = 0; t < lists.size(); ++t)
+                for (size_t j = 0; j < lists[t].size(); ++j) put(t + j * size_t(block), lists[t][j]);
+        } else {
+            otab.assign(4 * size_t(M), 0);
+            for (int k = 0; k < M; ++k) put(size_t(k), k);
+        }
+    }
+    const int32_t olen = int32_t(otab.size() / 4);
     auto up = [](size_t b) { return (b + 255) / 256 * 256; };
     const size_t b_tab = up(L.words * 8), b_sch = up(L.sched_words * 8), b_mis = up(md.size() * sizeof(MisalignDev));
-    const size_t b_poff = up(T.poff.size() * 4), b_pairs = up(T.pairs.size() * 4), b_err = 256;  // err + ops
+    const size_t b_otab = up(otab.size() * 4), b_pairs = up(T.pairs.size() * 4), b_err = 256;  // err + ops
     void* d_tab = nullptr;
-    int st = ctx_scratch(ctx, kTpsaScratchTable, b_tab + b_sch + b_mis + b_poff + b_pairs + b_err, &d_tab);
+    int st = ctx_scratch(ctx, kTpsaScratchTable, b_tab + b_sch + b_mis + b_otab + b_pairs + b_err, &d_tab);
     if (st != TP_OK) return st;
     char* base = static_cast<char*>(d_tab);
     double* dtable = reinterpret_cast<double*>(base);
     double* dsched = reinterpret_cast<double*>(base + b_tab);
     MisalignDev* dmis = reinterpret_cast<MisalignDev*>(base + b_tab + b_sch);
-    int32_t* dpoff = reinterpret_cast<int32_t*>(base + b_tab + b_sch + b_mis);
-    uint32_t* dpairs = reinterpret_cast<uint32_t*>(base + b_tab + b_sch + b_mis + b_poff);
-    int32_t* derr = reinterpret_cast<int32_t*>(base + b_tab + b_sch + b_mis + b_poff + b_pairs);
+    int4* dotab = reinterpret_cast<int4*>(base + b_tab + b_sch + b_mis);
+    uint32_t* dpairs = reinterpret_cast<uint32_t*>(base + b_tab + b_sch + b_mis + b_otab);
+    int32_t* derr = reinterpret_cast<int32_t*>(base + b_tab + b_sch + b_mis + b_otab + b_pairs);
     TPSA_CUDA(cudaMemcpyAsync(dtable, L.program, L.words * 8, cudaMemcpyHostToDevice, s));
     if (L.sched_words) TPSA_CUDA(cudaMemcpyAsync(dsched, L.sched, L.sched_words * 8, cudaMemcpyHostToDevice, s));
     if (!md.empty()) TPSA_CUDA(cudaMemcpyAsync(dmis, md.data(), md.size() * sizeof(MisalignDev), cudaMemcpyHostToDevice, s));
-    TPSA_CUDA(cudaMemcpyAsync(dpoff, T.poff.data(), T.poff.size() * 4, cudaMemcpyHostToDevice, s));
+    TPSA_CUDA(cudaMemcpyAsync(dotab, otab.data(), otab.size() * 4, cudaMemcpyHostToDevice, s));
     TPSA_CUDA(cudaMemcpyAsync(dpairs, T.pairs.data(), T.pairs.size() * 4, cudaMemcpyHostToDevice, s));
     unsigned long long* dops = reinterpret_cast<unsigned long long*>(reinterpret_cast<char*>(derr) + 16);
     TPSA_CUDA(cudaMemsetAsync(derr, 0, 48, s));
@@ -1079,11 +1151,6 @@ TP_API int tp_tpsa_ringpass(tp_ctx* ctx, const tp_lattice* lat, double* maps, in
     if ((st = ctx_scratch(ctx, kTpsaScratchMaps, map_bytes, &d_maps)) != TP_OK) return st;
     TPSA_CUDA(cudaMemcpyAsync(d_maps, maps, map_bytes, cudaMemcpyHostToDevice, s));
 
-    // launch shape: threads ~ M/2 (32..256); pool in shared memory when it fits
-    // about four coefficients per thread: enough work per operation to carry
-    // its barrier, and small CTAs so that registers allow 8 maps per SM
-    int block = (M / 4 + 31) / 32 * 32;
-    block = std::max(32, std::min(256, block));
     // series slots: the longer bodies hold more work series at once
     bool rare = L.nmis > 0;
     for (int32_t e = 0; e < L.nelem; ++e) {
@@ -1123,8 +1190,9 @@ TP_API int tp_tpsa_ringpass(tp_ctx* ctx, const tp_lattice* lat, double* maps, in
     a.sched_turn0 = L.sched_turn0;
     a.sched_nturns = L.sched_nturns;
     a.mis = md.empty() ? nullptr : dmis;
-    a.poff = dpoff;
+    a.otab = dotab;
     a.pairs = dpairs;
+    a.olen = olen;
     a.maps = static_cast<double*>(d_maps);
     a.nmaps = nmaps;
     a.gpool = gpool;
