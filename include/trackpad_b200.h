@@ -195,7 +195,9 @@ typedef struct tp_opts {
                                   5 % slower                                       */
     double aperture_x;         /* rectangular aperture half widths [m]; a value   */
     double aperture_y;         /* <= 0 disables it (reference limits remain)      */
-    void* stream;              /* cudaStream_t to run on; NULL = context stream   */
+    void* stream;              /* cudaStream_t to run on; NULL = context stream, a
+                                  blocking stream ordered with the legacy default
+                                  stream                                          */
 } tp_opts;
 
 /* Statistics of the last tracking call on a context. */

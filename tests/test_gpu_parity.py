@@ -207,6 +207,31 @@ def test_device_pointers_match_host_path():
     assert np.array_equal(dev.cpu().numpy().T, host) and np.array_equal(lost_d.cpu().numpy(), lost_h)
 
 
+@pytest.mark.parametrize("side_stream", [False, True])
+def test_device_inputs_filled_on_the_torch_stream_are_ordered(side_stream):
+    """Inputs written by PyTorch on its current stream (the default one, or a
+    side stream set with torch.cuda.stream) behind a ~25 ms kernel, then
+    tracked at once without a synchronize: the call must see the filled
+    inputs, not the NaN coordinates and set loss flags they replace."""
+    import torch
+    lat, beam = W.dba_ring(cells=2), W.dba_beam()
+    host = W.gaussian(4096, seed=8)
+    init = torch.from_numpy(np.ascontiguousarray(host.T)).cuda()
+    lost_h = np.zeros(4096, np.int64)
+    tp.ringpass_(host, lat, beam, lost_h, 3, aperture=0.02)
+    coords = torch.full_like(init, float("nan"))
+    lost = torch.ones(4096, dtype=torch.int64, device="cuda")
+    torch.cuda.synchronize()
+    side = torch.cuda.Stream() if side_stream else torch.cuda.current_stream()
+    with torch.cuda.stream(side):
+        torch.cuda._sleep(50_000_000)  # a bounded spin of 5e7 clock cycles
+        coords.copy_(init)
+        lost.zero_()
+        tp.ringpass_(coords.T, lat, beam, lost, 3, aperture=0.02)
+    torch.cuda.synchronize()
+    assert np.array_equal(coords.cpu().numpy().T, host) and np.array_equal(lost.cpu().numpy(), lost_h)
+
+
 def test_linearised_drift_option():
     lat, beam = W.fodo_ring(cells=2), W.fodo_beam()
     c = W.gaussian(256, seed=8)

@@ -466,7 +466,11 @@ TP_API int tp_ctx_create(int device, tp_ctx** out) {
     int optin = 0;
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     c->smem_optin = size_t(optin);
-    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    // A blocking stream: it waits for work queued on the legacy default stream
+    // and that stream waits for it, so device arrays a caller fills on its
+    // default stream (PyTorch's, unless it set another) are complete before a
+    // call's first kernel reads them.
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream, cudaStreamDefault);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
     if (e == cudaSuccess) e = cudaMalloc(&c->counters, 8 * sizeof(unsigned long long));

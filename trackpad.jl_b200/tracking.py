@@ -280,7 +280,14 @@ def spos(lat, time=0.0, turn=0):
 TABLE_IN_SMEM = False
 
 
-def _opts(aperture, exact, contract, device, block_size=0, schedule=0, stream=None):
+def _opts(aperture, exact, contract, device, block_size=0, schedule=0, stream=None, device_index=None):
+    """tp_opts of a call.  With device arrays and no stream given, the call runs
+    on PyTorch's current stream of that device, so the kernels follow the work
+    that wrote the inputs there; PyTorch's default stream has handle 0, which
+    selects the context stream, a blocking stream ordered with it."""
+    if device and stream is None:
+        import torch
+        stream = torch.cuda.current_stream(device_index).cuda_stream or None
     o = _abi.TpOpts()
     o.table_in_smem = 1 if TABLE_IN_SMEM else 0
     o.size = C.sizeof(_abi.TpOpts)
@@ -385,7 +392,7 @@ def ringpass_(coords, lat, beam, lost_flags, nturns, *, time=0.0, dt_turn=0.0, t
     b = _Buffers(coords, lost_flags, lost_turn, lost_elem)
     lat.set_schedule(time, dt_turn, turn, max(nturns, 1))
     dev = b.device_index if b.device else None
-    o = _opts(aperture, exact, contract, b.device, block_size, schedule, stream)
+    o = _opts(aperture, exact, contract, b.device, block_size, schedule, stream, device_index=dev)
     st = _abi.lib().tp_ringpass(context(dev), lat.handle, b.coords, b.n, b.lost, b.lost_turn, b.lost_elem,
                                 C.c_double(beti(beam)), nturns, C.c_double(time), C.c_double(dt_turn), int(turn),
                                 C.byref(o))
@@ -402,7 +409,7 @@ def linepass_(coords, lat, beam, lost_flags, *, time=0.0, turn=0, **kw):
     lat.set_schedule(time, 0.0, turn, 1)
     dev = b.device_index if b.device else None
     o = _opts(kw.get("aperture"), kw.get("exact", True), kw.get("contract", False), b.device, kw.get("block_size", 0),
-              kw.get("schedule", 0), kw.get("stream"))
+              kw.get("schedule", 0), kw.get("stream"), device_index=dev)
     st = _abi.lib().tp_linepass(context(dev), lat.handle, b.coords, b.n, b.lost, b.lost_turn, b.lost_elem,
                                 C.c_double(beti(beam)), C.c_double(time), int(turn), C.byref(o))
     _abi.check(st, "tp_linepass")
@@ -435,7 +442,8 @@ class Batch:
             raise ValueError("poff must have nvar+1 entries and betis nvar entries")
         if poff[-1] != b.n:
             raise ValueError("poff[-1] must equal the number of particles")
-        o = _opts(aperture, exact, contract, b.device, block_size, schedule, stream)
+        o = _opts(aperture, exact, contract, b.device, block_size, schedule, stream,
+                  device_index=b.device_index if b.device else None)
         st = _abi.lib().tp_ringpass_batched(context(self.device), self._handle, b.coords,
                                             poff.ctypes.data_as(C.c_void_p), b.lost, b.lost_turn, b.lost_elem,
                                             betis.ctypes.data_as(C.c_void_p), int(nturns), C.c_double(0.0),
@@ -466,7 +474,7 @@ class Batch:
         pof[1:] = np.cumsum([len(p) for p in params])
         loss = np.zeros(nv)
         grad = np.zeros(max(len(flat), 1))
-        o = _opts(aperture, exact, False, dev is not None, stream=stream)
+        o = _opts(aperture, exact, False, dev is not None, stream=stream, device_index=dev)
         ls = _loss_spec(sigma, lost_weight)
         st = _abi.lib().tp_ringpass_adjoint_batched(
             context(self.device), self._handle, cp, poff.ctypes.data_as(C.c_void_p), lp,
@@ -558,7 +566,7 @@ def ringpass_adjoint(coords0, lat, beam, lost0, nturns, params, *, sigma, lost_w
             out_c = torch.empty((6, n), dtype=torch.float64, device=f"cuda:{dev}").T
             out_l = torch.empty(n, dtype=torch.int64, device=f"cuda:{dev}")
             ocp, olp = C.c_void_p(out_c.data_ptr()), C.c_void_p(out_l.data_ptr())
-    o = _opts(aperture, exact, False, dev is not None, stream=stream)
+    o = _opts(aperture, exact, False, dev is not None, stream=stream, device_index=dev)
     ls = _loss_spec(sigma, lost_weight)
     st = _abi.lib().tp_ringpass_adjoint(context(dev), lat.handle, cp, n, lp, C.c_double(beti(beam)), int(nturns),
                                         C.c_double(time), C.c_double(dt_turn), int(turn),
