@@ -108,3 +108,27 @@ def test_fd_map_assembly_against_the_oracle():
     M = tp.optics.fd_assemble(c)
     R = oracle_ref.jacobian(lat, ref[None, :], tp.beti(beam))[0]
     assert np.abs(M - R).max() < 1e-6 * np.abs(R).max()
+
+
+def test_device_calls_run_on_the_callers_current_stream(monkeypatch):
+    """With device arrays and no stream given, tp_opts.stream is PyTorch's
+    current stream of the arrays' device; handle 0 (PyTorch's default stream)
+    becomes NULL, the context stream, which is ordered with it.  Host arrays
+    and an explicit stream are left as given."""
+    import torch
+
+    class _S:
+        def __init__(self, h):
+            self.cuda_stream = h
+
+    seen = []
+    handles = {None: 0, 3: 0xABC0}
+    monkeypatch.setattr(torch.cuda, "current_stream", lambda d=None: seen.append(d) or _S(handles[d]))
+    o = tp.tracking._opts(None, True, False, True, device_index=3)
+    assert o.stream == 0xABC0 and seen == [3]
+    o = tp.tracking._opts(None, True, False, True)
+    assert not o.stream
+    o = tp.tracking._opts(None, True, False, True, stream=0x55, device_index=3)
+    assert o.stream == 0x55 and seen == [3, None]
+    o = tp.tracking._opts(None, True, False, False)
+    assert not o.stream and seen == [3, None]
