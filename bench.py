@@ -40,8 +40,9 @@ SIGMA_LOSS = 1e-4      # sigma_x of the beam-size loss
 LOST_WEIGHT = 1e3
 
 # DRAM bytes per particle of one tracking launch: ncu capture of track_single on
-# the DBA ring, 69,632 particles x 10 turns (5.425 MB read + written).  Traffic
-# grows with the particle count (the table lives in shared memory).
+# the DBA ring, 135,168 particles (one full wave) x 10 turns, 1.407 GB read +
+# written, almost all of it the write-back of spilled stack lines.  Scaled by
+# the launch's particle count.
 DRAM_BYTES_PER_PARTICLE = 1.407376e9 / 135168
 
 

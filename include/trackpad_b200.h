@@ -430,7 +430,12 @@ TP_API int tp_one_turn_jacobian(tp_ctx* ctx, const tp_lattice* lat,
  *     misalignment rows or a per-turn schedule give TP_EUNSUPPORTED;
  *   * the array (about 128 KiB) stays allocated on every GPU that loads the
  *     library until the process exits, and every call shares it: calls that
- *     overlap on the GPU race with each other;
+ *     overlap on the GPU race with each other.  A call copies the element
+ *     table into the array only when the array does not already hold this
+ *     lattice's current program on that device; the kernel reads it through
+ *     the L1 cache, like tp_ringpass;
+ *   * the lattice must not be destroyed while a call on it runs (a schedule
+ *     change from another thread waits for the call's table copy);
  *   * the first call on a device looks up the array's address there; make it
  *     before any stream capture.
  * Always the exact drift and no FMA contraction (tp_opts defaults). */

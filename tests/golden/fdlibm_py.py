@@ -4,6 +4,16 @@ The golden-fixture generator evaluates the reference maps with these functions,
 the same method (and operation order) the CUDA kernels and the CPU oracle use,
 so that the fixtures, the oracle and the GPU agree bit for bit.  Python floats
 are IEEE binary64 and Python never fuses a multiply-add.
+
+The coefficient tables and branch structure follow fdlibm, whose routines carry
+this notice:
+
+    Copyright (C) 1993 by Sun Microsystems, Inc. All rights reserved.
+
+    Developed at SunPro, a Sun Microsystems, Inc. business.
+    Permission to use, copy, modify, and distribute this
+    software is freely granted, provided that this notice
+    is preserved.
 """
 import math
 import struct

@@ -56,6 +56,36 @@ def test_noalloc_matches_ringpass_on_two_calls_in_a_row():
     assert 0 < int(ref_lost.sum()) < n
 
 
+@pytest.mark.gpu
+def test_noalloc_switches_lattices():
+    """The array keeps the last call's element table: a call on another lattice
+    replaces it, and a call back on the first lattice restores it."""
+    import torch
+    beam = W.dba_beam()
+    lats = [W.dba_ring(cells=4), W.dba_ring(cells=3)]
+    host = np.concatenate([W.gaussian(1000, seed=22), W.da_grid(12, 12)])
+    n = len(host)
+    cols = torch.from_numpy(np.ascontiguousarray(host.T)).cuda()
+    refs = []
+    for lat in lats:
+        r = cols.clone()
+        rl = torch.zeros(n, dtype=torch.int64, device="cuda")
+        tp.ringpass_(r.T, lat, beam, rl, 3, aperture=0.02)
+        refs.append((r, rl))
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream().cuda_stream
+    for k in (0, 1, 0, 1):
+        c = cols.clone()
+        lost = torch.zeros(n, dtype=torch.int64, device="cuda")
+        lt = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+        le = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+        torch.cuda.synchronize()
+        st = _noalloc(lats[k], c, lost, lt, le, tp.beti(beam), 3, 0.02, stream)
+        assert st == abi.TP_OK, abi.lib().tp_last_error_string().decode()
+        torch.cuda.synchronize()
+        assert torch.equal(c, refs[k][0]) and torch.equal(lost, refs[k][1])
+
+
 def test_noalloc_rejects_tables_beyond_its_limit():
     # 1500 exact bends need more than the 16384-word table of the fixed array.
     lat = tp.Lattice([tp.ExactSBend(1.0, 0.01)] * 1500)

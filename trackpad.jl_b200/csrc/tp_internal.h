@@ -2,6 +2,7 @@
 #pragma once
 #include <stdint.h>
 
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -81,15 +82,20 @@ int launch_track_strict(const TrackArgs& a, int grid, int block, int ppt, size_t
 int occupancy_track_fast(int block, int ppt, size_t smem, int* blocks_per_sm);
 int occupancy_track_strict(int block, int ppt, size_t smem, int* blocks_per_sm);
 
-// Read-only view of a lattice's compiled program (tp_runtime.cu).
+// Read-only view of a lattice's compiled program (tp_runtime.cu).  The
+// program may be rebuilt by tp_lattice_set_schedule: hold lattice_mutex(lat)
+// while the view is used.  `stamp` is unique to this lattice and its current
+// program (every creation and every rebuild draws a new one).
 struct LatticeView {
     const double* program;  // host copy of the compiled table
     size_t words;
     int32_t nelem;
     bool has_schedule;
     bool has_misalignment;
+    uint64_t stamp;
 };
 void lattice_view(const tp_lattice* lat, LatticeView* out);
+std::mutex& lattice_mutex(const tp_lattice* lat);
 
 // Everything the adjoint and Jacobian paths read from a lattice (tp_runtime.cu).
 struct LatticeHost {

@@ -18,6 +18,16 @@
 // is checked against the C library (< 1 ulp) in the CPU tests.  Arguments
 // beyond the Cody-Waite range (|x| >= 2^20 * pi/2, only reachable by a particle
 // that is already lost) use the platform function.
+// The coefficient tables and branch structure below follow fdlibm, whose
+// routines carry this notice:
+//
+//   Copyright (C) 1993 by Sun Microsystems, Inc. All rights reserved.
+//
+//   Developed at SunPro, a Sun Microsystems, Inc. business.
+//   Permission to use, copy, modify, and distribute this
+//   software is freely granted, provided that this notice
+//   is preserved.
+//
 #pragma once
 #include <math.h>
 #include <stdint.h>

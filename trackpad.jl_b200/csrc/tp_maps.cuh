@@ -105,7 +105,34 @@ __device__ __forceinline__ void bend_kick(P6& s, const double* pa, const double*
     s.z = s.z + Kh * s.x * beti;
 }
 
-// symplectic4_pass (src/tracking.jl:317-341) for one multipole record.
+// drift6 (exact branch) with its NormL = L/sqrt(pz2) returned through `NormL`
+// (NaN when pz2 <= 0, where the state becomes NaN).
+__device__ __forceinline__ void drift_exact_norm(P6& s, double L, double Lbeti, const DCache& c, double& NormL) {
+    double pz2 = c.A - s.px * s.px - s.py * s.py;
+    if (pz2 <= 0.0) {
+        set_nan(s);
+        NormL = CUDART_NAN;
+        return;
+    }
+    NormL = L / sqrt(pz2);
+    s.x = s.x + NormL * s.px;
+    s.y = s.y + NormL * s.py;
+    s.z = s.z + NormL * c.bd - Lbeti;
+}
+
+// A second drift6 of the same length right after one (no kick between): px,
+// py and delta are unchanged, so pz2 and NormL = L/sqrt(pz2) are the previous
+// drift's bit for bit and only the position updates remain.  After a NaN drift
+// the state is NaN and stays NaN either way.
+__device__ __forceinline__ void drift_exact_again(P6& s, double NormL, double Lbeti, const DCache& c) {
+    s.x = s.x + NormL * s.px;
+    s.y = s.y + NormL * s.py;
+    s.z = s.z + NormL * c.bd - Lbeti;
+}
+
+// symplectic4_pass (src/tracking.jl:317-341) for one multipole record.  The
+// last drift D(L1) of a Yoshida step and the first D(L1) of the next follow
+// each other with no kick between, so the second reuses the first's NormL.
 template <int M, bool EXACT>
 __device__ __noinline__ void multipole(P6& s, const double* w, int nsteps, double beti) {
     const double L1 = w[mp::L1], L2 = w[mp::L2], K1 = w[mp::K1], K2 = w[mp::K2];
@@ -116,11 +143,17 @@ __device__ __noinline__ void multipole(P6& s, const double* w, int nsteps, doubl
     DCache c;
     make_cache(s, beti, c);
     // D(L1) K(K1) D(L2) K(K2) D(L2) K(K1) D(L1) per step, as one loop (code size).
+    double carry = 0.0;
 #pragma unroll 1
     for (int k = 0; k < 4 * nsteps; ++k) {
         const int j = k & 3;
         const bool outer = (j == 0) || (j == 3);
-        drift<EXACT>(s, outer ? L1 : L2, outer ? L1b : L2b, c);
+        if (EXACT) {
+            if (j == 0 && k > 0) drift_exact_again(s, carry, L1b, c);
+            else drift_exact_norm(s, outer ? L1 : L2, outer ? L1b : L2b, c, carry);
+        } else {
+            drift<EXACT>(s, outer ? L1 : L2, outer ? L1b : L2b, c);
+        }
         if (j != 3) thin_kick<M>(s, pa, pb, j == 1 ? K2 : K1);
     }
 }
@@ -161,14 +194,19 @@ __device__ __noinline__ void sbend(P6& s, const double* w, const RecHdr& h, doub
     const double K1h = K1 * irho, K2h = K2 * irho;
     DCache c;
     make_cache(s, beti, c);
+    // As in multipole(): a step's first D(L1) reuses the previous step's last.
+    double carry = 0.0;
     for (int st = 0; st < h.nsteps; ++st) {
-        drift<EXACT>(s, L1, L1b, c);
+        if (!EXACT) drift<EXACT>(s, L1, L1b, c);
+        else if (st > 0) drift_exact_again(s, carry, L1b, c);
+        else drift_exact_norm(s, L1, L1b, c, carry);
         bend_kick<M>(s, pa, pb, K1, K1h, irho, beti);
         drift<EXACT>(s, L2, L2b, c);
         bend_kick<M>(s, pa, pb, K2, K2h, irho, beti);
         drift<EXACT>(s, L2, L2b, c);
         bend_kick<M>(s, pa, pb, K1, K1h, irho, beti);
-        drift<EXACT>(s, L1, L1b, c);
+        if (EXACT) drift_exact_norm(s, L1, L1b, c, carry);
+        else drift<EXACT>(s, L1, L1b, c);
     }
     if (h.flags & RF_FRINGE_OUT)
         edge_fringe(s, irho, w[sb::FX_OUT], w[sb::E_OUT], w[sb::FC_OUT], h.method_out, h.flags & RF_FC_OUT_ZERO, true);

@@ -19,8 +19,11 @@
 //   * every GPU that loads the library holds the array (about 128 KiB) until
 //     the process exits;
 //   * every call shares the array: the counters and the error word are cleared
-//     at the start of each call and the table is overwritten, so calls that
-//     overlap on the GPU race with each other;
+//     at the start of each call, and the table is overwritten whenever the
+//     call's lattice (or its program) differs from the one the array holds on
+//     that device, so calls that overlap on the GPU race with each other;
+//   * the kernel reads the table from the array through the L1 cache (every
+//     lane of a warp reads the same record word), as tp_ringpass does;
 //   * the first call on a device looks up the array's device address there
 //     (cudaGetSymbolAddress); make that first call before any stream capture.
 #include <cuda_runtime.h>
@@ -40,12 +43,12 @@ constexpr int kScratchWords = kHeadWords + kNoAllocTableWords;
 constexpr int kMaxDev = 16;
 
 // The allocation-free scratch: words [0, 4) counters (work, passes), [4, 8)
-// error word, [32, 32 + 16384) element table (16-byte aligned for the bulk
-// copy into shared memory).
+// error word, [32, 32 + 16384) element table (256-byte aligned).
 static __device__ __align__(256) double g_noalloc_scratch[kScratchWords];
 
-std::mutex g_mu;
+std::mutex g_mu;                      // serialises the set-up of the calls of this process
 double* g_scratch_dev[kMaxDev] = {};  // device address of the array on each device
+uint64_t g_resident[kMaxDev] = {};    // lattice stamp whose table the array holds (0: none)
 
 int fail(int st, const std::string& msg) {
     tp::set_last_error(msg);
@@ -65,6 +68,9 @@ TP_API int tp_ringpass_noalloc(const tp_lattice* lat, double* coords, int64_t n,
     if (n < 0 || nturns < 0) return fail(TP_EINVAL, "negative particle count or number of turns");
     if (!(beti > 0.0) || !std::isfinite(beti)) return fail(TP_EINVAL, "beti must be finite and positive");
     if (n > 0 && (!coords || !lost_flags)) return fail(TP_EINVAL, "coords and lost_flags are required");
+    // The lattice's program may be rebuilt by tp_lattice_set_schedule: hold
+    // its lock while the program is read and copied.
+    std::unique_lock<std::mutex> lat_lock(tp::lattice_mutex(lat));
     tp::LatticeView v;
     tp::lattice_view(lat, &v);
     if (v.has_schedule || v.has_misalignment)
@@ -78,34 +84,40 @@ TP_API int tp_ringpass_noalloc(const tp_lattice* lat, double* coords, int64_t n,
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
     if (dev < 0 || dev >= kMaxDev) return fail(TP_EINVAL, "device ordinal out of range");
-    double* scratch = nullptr;
-    {
-        std::lock_guard<std::mutex> g(g_mu);
-        if (!g_scratch_dev[dev]) {
-            // Once per device, with that device current: the array's device address.
-            void* p = nullptr;
-            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress");
-            g_scratch_dev[dev] = static_cast<double*>(p);
-        }
-        scratch = g_scratch_dev[dev];
-    }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    double* scratch = nullptr;
+    std::unique_lock<std::mutex> g(g_mu);
+    if (!g_scratch_dev[dev]) {
+        // Once per device, with that device current: the array's device address.
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress");
+        g_scratch_dev[dev] = static_cast<double*>(p);
+    }
+    scratch = g_scratch_dev[dev];
     int sm = 0;
     e = cudaDeviceGetAttribute(&sm, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceGetAttribute");
 
-    // Clear what must start at zero; overwrite the table.
+    // Clear what must start at zero; copy the table unless this lattice's
+    // current program is the one the array already holds on this device.
     e = cudaMemsetAsync(scratch, 0, kHeadWords * sizeof(double), s);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(scratch + kHeadWords, v.program, v.words * sizeof(double), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return cuda_fail(e, "scratch set-up");
+    if (g_resident[dev] != v.stamp) {
+        g_resident[dev] = 0;
+        e = cudaMemcpyAsync(scratch + kHeadWords, v.program, v.words * sizeof(double), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) return cuda_fail(e, "element table copy");
+        g_resident[dev] = v.stamp;
+    }
+    const bool rare = tp::records_have_rare(v.program, v.words);
+    g.unlock();
+    lat_lock.unlock();
 
     tp::TrackArgs a{};
     a.table = scratch + kHeadWords;
     a.table_words = int32_t(v.words);
     a.nelem = v.nelem;
-    a.rare = tp::records_have_rare(v.program, v.words) ? 1 : 0;
+    a.rare = rare ? 1 : 0;
     a.coords = coords;
     a.n = n;
     a.lost_flags = lost_flags;
@@ -121,8 +133,8 @@ TP_API int tp_ringpass_noalloc(const tp_lattice* lat, double* coords, int64_t n,
     a.work = reinterpret_cast<unsigned long long*>(scratch);
     a.passes = reinterpret_cast<unsigned long long*>(scratch) + 1;
     a.err = reinterpret_cast<int32_t*>(scratch + 4);
-    a.smem_words = int32_t(v.words);
-    const size_t smem = v.words * sizeof(double);
+    a.smem_words = 0;  // the table is read through the L1 cache, as tp_ringpass does by default
+    const size_t smem = 0;
     const int block = 128;
     int bps = 0;
     if (tp::occupancy_track_strict(block, 1, smem, &bps) != 0 || bps <= 0) bps = 1;

@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -80,6 +81,9 @@ void tune_record(SchedTune& t, uint64_t key, int schedule, float ms) {
     if (++t.trials == 2) t.best = t.ms[1] < t.ms[0] ? 2 : 1;
 }
 
+std::atomic<uint64_t> g_stamp{0};
+uint64_t next_stamp() { return ++g_stamp; }
+
 // Device copy of a lattice on one device.
 struct DevLattice {
     double* table = nullptr;
@@ -109,6 +113,7 @@ struct tp_lattice {
     int32_t sched_stride = 0;
     bool has_sched = false;
     uint64_t version = 1;
+    uint64_t stamp = next_stamp();     // unique per lattice and program (see LatticeView)
     DevLattice dev[kMaxDevices];
     std::mutex mu;
 };
@@ -137,14 +142,10 @@ struct tp_batch {
     unsigned long long* pool = nullptr; // per variant particles handed out (pooled refill)
     SchedTune tune;
     std::vector<int64_t> h_sched_v;
-    // cached CUDA graph of the launch sequence
+    // cached CUDA graph of the launch sequence and every value it bakes in
+    // (argument values, device pointers, launch shapes; see graph_key)
     cudaGraphExec_t graph = nullptr;
-    std::vector<int64_t> g_poff;
-    int32_t g_nturns = -1, g_turn0 = 0, g_exact = -1, g_strict = -1, g_refill = -1;
-    double g_limx = 0, g_limy = 0;
-    const void* g_coords = nullptr;
-    const void* g_lost = nullptr;
-    const void* g_table = nullptr;
+    std::vector<uint64_t> g_key;
 };
 
 struct tp_ctx {
@@ -357,7 +358,10 @@ void lattice_view(const tp_lattice* lat, LatticeView* out) {
     out->nelem = int32_t(lat->elems.size());
     out->has_schedule = lat->has_sched;
     out->has_misalignment = !lat->mis.empty();
+    out->stamp = lat->stamp;
 }
+
+std::mutex& lattice_mutex(const tp_lattice* lat) { return const_cast<tp_lattice*>(lat)->mu; }
 
 void lattice_host(const tp_lattice* lat, LatticeHost* out) {
     out->elems = lat->elems.data();
@@ -595,6 +599,7 @@ TP_API int tp_lattice_set_schedule(tp_lattice* L, const int32_t* fields, int32_t
         L->has_sched = false;
         L->sfields.clear(); L->svalues.clear(); L->sched_table.clear();
         L->version++;
+        L->stamp = next_stamp();
         return TP_OK;
     }
     if (nfields < 0 || !fields || nturns <= 0 || !values) return set_err(TP_EINVAL, "bad schedule arguments");
@@ -647,6 +652,7 @@ TP_API int tp_lattice_set_schedule(tp_lattice* L, const int32_t* fields, int32_t
     L->sched_stride = stride;
     L->has_sched = true;
     L->version++;
+    L->stamp = next_stamp();
     return TP_OK;
 }
 
@@ -1127,14 +1133,25 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
         return TP_OK;
     };
     if (use_graph) {
-        // The graph bakes in the argument values; rebuild it when they change.
-        bool same = b->graph && b->g_nturns == nturns && b->g_turn0 == turn0 && b->g_exact == int(exact) &&
-                    b->g_strict == int(strict) && b->g_limx == a.limx && b->g_limy == a.limy &&
-                    b->g_coords == d_coords && b->g_lost == d_lost && b->g_table == b->table &&
-                    b->g_refill == a.refill &&
-                    b->g_poff == std::vector<int64_t>(poff, poff + nvar + 1);
-        if (!same) {
+        // The graph bakes in every value the sequence reads on the host: the
+        // kernels' arguments (the context's counters, error word, FLOP
+        // accumulator and alive mask; the coordinate, flag and loss-record
+        // arrays; the batch's tables), which of the fill kernels run, and the
+        // launch shapes.  Any change rebuilds it.
+        auto u = [](const void* p) { return uint64_t(reinterpret_cast<uintptr_t>(p)); };
+        auto dbits = [](double x) { uint64_t r; std::memcpy(&r, &x, sizeof r); return r; };
+        std::vector<uint64_t> key = {
+            u(c), u(c->counters), u(c->err), u(c->flops_acc), u(c->alive0), uint64_t(c->cap),
+            u(d_coords), u(d_lost), u(d_lt), u(d_le), uint64_t(dev && lost_turn), uint64_t(dev && lost_elem),
+            u(b->table), u(b->toff), u(b->poff), u(b->beti_v), u(b->nelem_v), u(b->mis), u(b->sched),
+            u(b->sched_v), u(b->pool), u(b->prefix), u(b->prefix_off), u(d_pre),
+            uint64_t(uint32_t(nturns)), uint64_t(uint32_t(turn0)), uint64_t(exact), uint64_t(strict),
+            uint64_t(a.refill), uint64_t(a.rare), dbits(a.limx), dbits(a.limy), dbits(a.beti),
+            uint64_t(block), uint64_t(grid), uint64_t(sg), uint64_t(n)};
+        for (int32_t v = 0; v <= nvar; ++v) key.push_back(uint64_t(poff[v]));
+        if (!b->graph || b->g_key != key) {
             if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+            b->g_key.clear();
             cudaStream_t cap = nullptr;
             TP_CUDA(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
             TP_CUDA(cudaStreamSynchronize(s));
@@ -1148,11 +1165,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
             ce = cudaGraphInstantiate(&b->graph, graph, 0);
             cudaGraphDestroy(graph);
             if (ce != cudaSuccess) { b->graph = nullptr; return cuda_err(ce, "cudaGraphInstantiate"); }
-            b->g_nturns = nturns; b->g_turn0 = turn0; b->g_exact = int(exact); b->g_strict = int(strict);
-            b->g_limx = a.limx; b->g_limy = a.limy; b->g_coords = d_coords; b->g_lost = d_lost;
-            b->g_table = b->table;
-            b->g_refill = a.refill;
-            b->g_poff.assign(poff, poff + nvar + 1);
+            b->g_key.swap(key);
         }
         TP_CUDA(cudaEventRecord(c->ev0, s));
         TP_CUDA(cudaGraphLaunch(b->graph, s));

@@ -1,11 +1,13 @@
 // tp_track.cu -- the tracking kernel (ringpass!/linepass! on the device).
 //
 // One thread per particle; the 6D FP64 state stays in registers across every
-// element and turn of the launch.  The compiled element table is staged into
-// shared memory once per block with a TMA bulk copy (cp.async.bulk, no
-// multicast) completed on an mbarrier; every lane of a warp then reads the
-// same record (broadcast).  Particles are read and written in coalesced SoA
-// order (column c of the N x 6 column-major array).
+// element and turn of the launch.  Every lane of a warp reads the same word of
+// the compiled element table at the same time (a broadcast); by default the
+// table is read through the L1 cache, where it stays resident.  On request
+// (TrackArgs::smem_words > 0) each block first stages it into shared memory
+// with a bulk copy (cp.async.bulk, no multicast) completed on an mbarrier.
+// Particles are read and written in coalesced SoA order (column c of the N x 6
+// column-major array).
 //
 // Scheduling.  With lane refill a persistent warp takes particle indices from
 // a global counter (one warp-aggregated atomic per refill); a lane whose
@@ -34,9 +36,7 @@ namespace TP_NS {
 
 using namespace tp::dev;
 
-// 128-thread blocks, at least 5 resident per SM: at most 102 registers per
-// thread (measured fastest on B200 among 128/4, 128/5, 128/6, 128/8 and
-// 64/256-thread blocks; fewer registers spill in the exact-bend maps).
+// 128-thread blocks (64- and 256-thread blocks measured slower).
 #ifndef TP_MAX_BLOCK
 #define TP_MAX_BLOCK 128
 #endif
@@ -119,13 +119,19 @@ __device__ __forceinline__ bool is_lost(const P6& s, double limx, double limy) {
     return isnan(s.x) || fabs(s.x) > limx || fabs(s.y) > limy || fabs(s.px) > 1.0 || fabs(s.py) > 1.0;
 }
 
+// The per-turn table of a lattice's scheduled elements.
+struct SchedView {
+    const double* p;
+    int32_t stride, turn0, nturns;
+};
+
 // Header of the record to use at `turn` (scheduled elements live in the
 // per-turn table).  Returns null when the turn is outside the schedule.
-__device__ __forceinline__ const double* resolve(const double* rec, RecHdr& h, const TrackArgs& a, int turn) {
+__device__ __forceinline__ const double* resolve(const double* rec, RecHdr& h, const SchedView& sv, int turn) {
     if (!(h.flags & RF_SCHEDULED)) return rec;
-    int row = turn - a.sched_turn0;
-    if (row < 0 || row >= a.sched_nturns) return nullptr;
-    const double* p = a.sched + int64_t(row) * a.sched_stride + h.aux;
+    int row = turn - sv.turn0;
+    if (row < 0 || row >= sv.nturns) return nullptr;
+    const double* p = sv.p + int64_t(row) * sv.stride + h.aux;
     h = *reinterpret_cast<const RecHdr*>(p);
     return p;
 }
@@ -134,7 +140,8 @@ __device__ __forceinline__ const double* resolve(const double* rec, RecHdr& h, c
 // (`nelem` records).  Slot state is per lane.  With REFILL, lanes take new
 // particles from `next_particle` at turn boundaries until it returns < 0.
 template <bool EXACT, bool REFILL, bool RARE, typename NextFn>
-__device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, double beti, NextFn next_particle) {
+__device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, double beti, const SchedView& sv,
+                         NextFn next_particle) {
     const double beta = 1.0 / beti;
     const double beta2 = beta * beta;
     const int lane = threadIdx.x & 31;
@@ -175,7 +182,7 @@ __device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, doubl
             if (__ballot_sync(0xffffffffu, act) == 0) break;
             if (act) {
                 RecHdr h = h0;
-                const double* r = resolve(rec, h, a, a.turn0 + t);
+                const double* r = resolve(rec, h, sv, a.turn0 + t);
                 if (r == nullptr) {
                     atomicOr(a.err, DE_SCHED_RANGE);
                     act = false;
@@ -214,6 +221,7 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_single(TrackAr
     extern __shared__ __align__(16) double smem[];
     __shared__ __align__(8) uint64_t mbar;
     const double* tab = a.table;
+    const SchedView sv{a.sched, a.sched_stride, a.sched_turn0, a.sched_nturns};
     if (a.smem_words > 0) {
         if (!stage_table(smem, a.table, a.smem_words, &mbar)) {
             if (threadIdx.x == 0) atomicOr(a.err, DE_TMA_TIMEOUT);
@@ -232,14 +240,14 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_single(TrackAr
             unsigned long long j = base + __popc(need & ((1u << lane) - 1u));
             return j < (unsigned long long)a.n ? int64_t(j) : -1;
         };
-        run_warp<EXACT, true, RARE>(a, tab, a.nelem, a.beti, next);
+        run_warp<EXACT, true, RARE>(a, tab, a.nelem, a.beti, sv, next);
     } else {
         const int64_t gid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
         auto next = [&](unsigned need, int lane, bool& more) -> int64_t {
             more = false;
             return gid < a.n ? gid : -1;
         };
-        run_warp<EXACT, false, RARE>(a, tab, a.nelem, a.beti, next);
+        run_warp<EXACT, false, RARE>(a, tab, a.nelem, a.beti, sv, next);
     }
 }
 
@@ -287,17 +295,15 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_batched(TrackA
             const unsigned long long j = base + __popc(need & ((1u << ln) - 1u));
             return j < nv ? p0 + int64_t(j) : -1;
         };
+        // this variant's per-turn schedule (none: no record of the variant is scheduled)
+        SchedView sv{nullptr, 0, 0, 0};
         if (a.sched_v != nullptr && a.sched_v[4 * v] >= 0) {
-            // this variant's per-turn schedule
-            TrackArgs av = a;
-            av.sched = a.sched + a.sched_v[4 * v];
-            av.sched_stride = int32_t(a.sched_v[4 * v + 1]);
-            av.sched_turn0 = int32_t(a.sched_v[4 * v + 2]);
-            av.sched_nturns = int32_t(a.sched_v[4 * v + 3]);
-            run_warp<EXACT, REFILL, RARE>(av, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next);
-        } else {
-            run_warp<EXACT, REFILL, RARE>(a, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], next);
+            sv.p = a.sched + a.sched_v[4 * v];
+            sv.stride = int32_t(a.sched_v[4 * v + 1]);
+            sv.turn0 = int32_t(a.sched_v[4 * v + 2]);
+            sv.nturns = int32_t(a.sched_v[4 * v + 3]);
         }
+        run_warp<EXACT, REFILL, RARE>(a, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], sv, next);
     }
 }
 
