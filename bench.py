@@ -6,8 +6,12 @@ electrons, 401 elements (20 cells + RF), 1,048,576 Gaussian particles plus a
 512 x 512 dynamic-aperture grid, rectangular aperture 0.02 m.  One step is
 ringpass! over STEP_TURNS turns of that whole beam, restarted from the input
 distribution.  Synthetic, seeded inputs (Philox); no dataset is involved.  The
-default line also carries the adjoint/forward time ratio of the gradient
-workload (65,536 particles, 256 turns, 120 k1 + 80 k2).
+default line also carries, under the same clock: the adjoint/forward time
+ratio of the gradient workload (65,536 particles, 256 turns, 120 k1 + 80 k2;
+key "adjoint"), the batched forward workload (256 variants, 100-turn steps,
+its roofline fraction and its speed-up over the plain tracker run lattice by
+lattice; key "batched") and the batched time-dependent adjoint / batched
+forward time ratio (64 variants, 50-turn steps; key "batched_adjoint").
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--workload dba|fodo|batched|adjoint|batched_adjoint]
@@ -66,6 +70,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-adjoint", action="store_true", help="default workload: skip the adjoint ratio")
+    p.add_argument("--no-batched", action="store_true",
+                   help="default workload: skip the batched forward and batched adjoint summaries")
     return p.parse_args()
 
 
@@ -159,6 +165,15 @@ def batched_workload(args, rank, time_dependent=False):
                 beam=W.dba_beam(), aperture=0.02, turns=turns)
 
 
+def cpu_baselines(w):
+    """The all-core figure (OpenMP over particles) and, beside it, one host
+    thread: the reference's own ringpass! is single-threaded."""
+    allc = cpu_baseline(w)
+    one = cpu_baseline(w, target_s=5.0, chunk=128, threads=1)
+    allc["single_thread"] = {"value": one["value"], "unit": one["unit"], "cores": 1, "sample": one["sample"]}
+    return allc
+
+
 def cpu_baseline(w, target_s=10.0, chunk=1024, threads=0):
     """The oracle (C++ restatement of the reference loop order: elements outer,
     particles inner, OpenMP over particles) on the host cores, on successive
@@ -195,17 +210,21 @@ def run_reference(args):
     __graft_entry__.load_package()
     w = workload(args, 0)
     # Each step is a bounded sample of the workload: ~4 s of CPU work.
-    vals = []
+    vals, step_ms = [], []
     base = None
     for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
         r = cpu_baseline(w, target_s=4.0 if i >= args.warmup else 0.5)
+        dt = time.perf_counter() - t0
         if i >= args.warmup:
             vals.append(r["value"])
+            step_ms.append(dt * 1e3)
         base = r
     v = float(np.median(vals))
     line = {"impl": "reference", "metric": "particle*element*turns/s FP64", "value": v,
             "unit": "particle*element*turns/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": 4000.0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "ms_per_step": float(np.mean(step_ms)), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded Philox Gaussian beam + DA grid)",
             "config": {"workload": w["name"], "step": f"about 4 s of {w['turns']}-turn chunks of the beam per step"},
             "cpu_baseline": {"value": v, "unit": base["unit"], "cores": base["cores"], "kind": "port",
@@ -346,10 +365,15 @@ def main_track(args, tp, torch, rank, world, local, dist):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(w)
-    adj = None
+        cpu = cpu_baselines(w)
+    adj = bat = bat_adj = None
     if args.workload == "dba" and world == 1 and not args.no_adjoint:
         adj = adjoint_ratio(tp, local)
+    if args.workload == "dba" and world == 1 and not args.no_batched:
+        # the batched forward (256 variants, 100-turn steps) and the batched
+        # time-dependent adjoint ratio, under the same clock as the headline
+        bat = batched_summary(args, tp, torch, local)
+        bat_adj = batched_adjoint_summary(args, tp, torch, local)
 
     if rank == 0:
         line = {
@@ -372,14 +396,19 @@ def main_track(args, tp, torch, rank, world, local, dist):
         }
         if adj is not None:
             line["adjoint"] = adj
+        if bat is not None:
+            line["batched"] = bat
+        if bat_adj is not None:
+            line["batched_adjoint"] = bat_adj
         print(json.dumps(line))
 
 
 # ---------------------------------------------------------------------------
 # Batched forward tracking
 # ---------------------------------------------------------------------------
-def main_batched(args, tp, torch, rank, world, local, dist):
-    w = batched_workload(args, rank)
+def batched_measure(w, tp, torch, local, steps, warmup, dist=None):
+    """Device-timed batched forward steps of workload `w` (inputs resident in
+    HBM, one CUDA-graph launch per step, L2 flushed between steps)."""
     dev = torch.device("cuda", local)
     n = w["coords"].shape[0]
     batch = tp.Batch(w["lats"], device=local)
@@ -401,7 +430,7 @@ def main_batched(args, tp, torch, rank, world, local, dist):
         flush.fill_(1)
         return st
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     torch.cuda.synchronize()
     if dist:
@@ -411,7 +440,7 @@ def main_batched(args, tp, torch, rank, world, local, dist):
     e1 = torch.cuda.Event(enable_timing=True)
     kernel_ms, flops, units, launches = [], 0.0, 0.0, 0
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         st = step()
         kernel_ms.append(st["kernel_ms"])
         flops += st["flops"]
@@ -421,34 +450,67 @@ def main_batched(args, tp, torch, rank, world, local, dist):
     torch.cuda.synchronize()
     clk = clocks.stop()
     elapsed = e0.elapsed_time(e1) / 1e3
-    t = torch.tensor([elapsed, units], dtype=torch.float64, device=dev)
+    return dict(batch=batch, betis=betis, init=init, sptr=sptr, elapsed=elapsed, units=units, flops=flops,
+                kernel_ms=float(np.mean(kernel_ms)), launches=launches, st=st, clocks=clk)
+
+
+def lattice_by_lattice(w, m, tp, torch, local, nsample=16):
+    """The plain tracker run lattice by lattice on the same beams (a sample of
+    variants, same turns): what batching replaces."""
+    dev = torch.device("cuda", local)
+    u, tms = 0.0, 0.0
+    nsample = min(nsample, len(w["lats"]))
+    for v in range(nsample):
+        s = slice(int(w["poff"][v]), int(w["poff"][v + 1]))
+        c = m["init"][:, s].contiguous()
+        l = torch.zeros(c.shape[1], dtype=torch.int64, device=dev)
+        for _rep in range(2):
+            c.copy_(m["init"][:, s])
+            l.zero_()
+            tp.ringpass_(c.T, w["lats"][v], w["beam"], l, w["turns"], aperture=w["aperture"], stream=m["sptr"])
+            stv = tp.last_stats(local)
+        u += stv["units"]
+        tms += stv["kernel_ms"]
+    return {"value": u / (tms * 1e-3), "unit": "particle*element*turns/s",
+            "sample": f"the first {nsample} variants, one ringpass! launch each, device time"}
+
+
+def batched_summary(args, tp, torch, local):
+    """The batched forward workload (256 DBA variants, 100-turn steps) as an
+    object of the default line."""
+    w = batched_workload(argparse.Namespace(nvar=0, turns=0), 0)
+    m = batched_measure(w, tp, torch, local, steps=3, warmup=3)
+    peak = tp.probe_fp64_peak(local)
+    achieved = (m["flops"] / 3) / (m["kernel_ms"] * 1e-3) / 1e12
+    value = m["units"] / m["elapsed"]
+    lbl = lattice_by_lattice(w, m, tp, torch, local)
+    return {"metric": "particle*element*turns/s FP64 (batched)", "value": value, "unit": "particle*element*turns/s",
+            "steps": 3, "warmup": 3, "ms_per_step": m["elapsed"] / 3 * 1e3,
+            "config": {"workload": w["name"], "turns_per_step": w["turns"],
+                       "particles": int(w["coords"].shape[0]),
+                       "schedule": {1: "static tiles", 2: "pooled refill"}.get(m["st"]["schedule"]),
+                       "survivors": m["st"]["survivors"], "l2": "flushed between timed steps (256 MiB write)"},
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "kernel_ms": m["kernel_ms"],
+                         "peak_source": "measured FP64 FMA throughput of this device (tp_probe_fp64_peak)"},
+            "lattice_by_lattice": lbl, "speedup_vs_lattice_by_lattice": value / lbl["value"],
+            "target": ">= 0.5 of the FP64 peak", "clocks": m["clocks"]}
+
+
+def main_batched(args, tp, torch, rank, world, local, dist):
+    w = batched_workload(args, rank)
+    n = w["coords"].shape[0]
+    m = batched_measure(w, tp, torch, local, args.steps, args.warmup, dist)
+    t = torch.tensor([m["elapsed"], m["units"]], dtype=torch.float64, device=torch.device("cuda", local))
     if dist:
         dist.all_reduce(t[0:1], op=dist.ReduceOp.MAX)
         dist.all_reduce(t[1:2], op=dist.ReduceOp.SUM)
     elapsed, units_all = float(t[0]), float(t[1])
     peak = tp.probe_fp64_peak(local)
-    k_ms = float(np.mean(kernel_ms))
-    achieved = (flops / args.steps) / (k_ms * 1e-3) / 1e12
-
-    # The plain tracker run lattice by lattice on the same beams (a sample of
-    # variants, same turns): what batching replaces.
-    lbl = None
-    if rank == 0:
-        nsample = min(16, len(w["lats"]))
-        u, tms = 0.0, 0.0
-        for v in range(nsample):
-            s = slice(int(w["poff"][v]), int(w["poff"][v + 1]))
-            c = init[:, s].contiguous()
-            l = torch.zeros(c.shape[1], dtype=torch.int64, device=dev)
-            for rep in range(2):
-                c.copy_(init[:, s])
-                l.zero_()
-                tp.ringpass_(c.T, w["lats"][v], w["beam"], l, turns, aperture=w["aperture"], stream=sptr)
-                stv = tp.last_stats(local)
-            u += stv["units"]
-            tms += stv["kernel_ms"]
-        lbl = {"value": u / (tms * 1e-3), "unit": "particle*element*turns/s",
-               "sample": f"the first {nsample} variants, one ringpass! launch each, device time"}
+    achieved = (m["flops"] / args.steps) / (m["kernel_ms"] * 1e-3) / 1e12
+    st = m["st"]
+    lbl = lattice_by_lattice(w, m, tp, torch, local) if rank == 0 else None
+    batch, betis, turns = m["batch"], m["betis"], w["turns"]
 
     e2e = None
     if not args.no_e2e:
@@ -491,8 +553,9 @@ def main_batched(args, tp, torch, rank, world, local, dist):
                          "frac": achieved / peak, "traffic": DRAM_BYTES_PER_PARTICLE * n,
                          "traffic_source": "per-particle DRAM bytes of the single-lattice capture, scaled",
                          "peak_source": "measured FP64 FMA throughput of this device (tp_probe_fp64_peak)",
-                         "flops_per_launch": flops / args.steps, "kernel_ms": k_ms},
-            "lattice_by_lattice": lbl, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+                         "flops_per_launch": m["flops"] / args.steps, "kernel_ms": m["kernel_ms"]},
+            "lattice_by_lattice": lbl, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": m["launches"],
+            "clocks": m["clocks"],
         }
         print(json.dumps(line))
 
@@ -529,8 +592,9 @@ def main_adjoint(args, tp, torch, rank, world, local, dist):
         print(json.dumps(line))
 
 
-def main_batched_adjoint(args, tp, torch, rank, world, local, dist):
-    w = batched_workload(args, rank, time_dependent=True)
+def batched_adjoint_measure(w, tp, torch, local, steps, warmup):
+    """Per step: the batched forward (CUDA graph) and the batched adjoint
+    (loss and gradients of every variant) on the same beams; device times."""
     import trackpad_b200.workloads as W
     dev = torch.device("cuda", local)
     n = w["coords"].shape[0]
@@ -544,33 +608,54 @@ def main_batched_adjoint(args, tp, torch, rank, world, local, dist):
     stream = torch.cuda.current_stream(dev)
     clocks = Clocks(local)
     fwd, adj, rev = [], [], []
-    for i in range(max(1, min(args.warmup, 2)) + args.steps):
+    st = None
+    for i in range(warmup + steps):
         coords.copy_(init)
         lost.zero_()
         batch.ringpass_(coords.T, w["poff"], betis, lost, turns, aperture=w["aperture"], use_graph=True,
                         stream=stream.cuda_stream)
         f = tp.last_stats(local)["kernel_ms"]
-        loss, grads = batch.ringpass_adjoint(init.T, w["poff"], betis, None, turns, params, sigma=SIGMA_LOSS,
-                                             lost_weight=LOST_WEIGHT, aperture=w["aperture"])
+        batch.ringpass_adjoint(init.T, w["poff"], betis, None, turns, params, sigma=SIGMA_LOSS,
+                               lost_weight=LOST_WEIGHT, aperture=w["aperture"])
         st = tp.adjoint_stats()
-        if i >= max(1, min(args.warmup, 2)):
+        if i >= warmup:
             fwd.append(f)
             adj.append(st["forward_ms"] + st["reverse_ms"])
             rev.append(st["reverse_ms"])
     clk = clocks.stop()
     f, a = float(np.median(fwd)), float(np.median(adj))
+    return dict(f=f, a=a, rev=float(np.median(rev)), st=st, clocks=clk, params=int(sum(len(p) for p in params)))
+
+
+def batched_adjoint_summary(args, tp, torch, local):
+    """The batched time-dependent adjoint / batched forward time ratio (64
+    variants, 16,384 particles each, 50-turn steps) as an object of the
+    default line."""
+    w = batched_workload(argparse.Namespace(nvar=0, turns=0), 0, time_dependent=True)
+    m = batched_adjoint_measure(w, tp, torch, local, steps=2, warmup=1)
+    return {"metric": "batched adjoint/forward time ratio", "value": m["a"] / m["f"], "unit": "x",
+            "higher_is_better": False, "steps": 2, "warmup": 1,
+            "config": {"workload": w["name"], "turns_per_step": w["turns"], "parameters": m["params"]},
+            "batched_forward_ms": m["f"], "batched_adjoint_ms": m["a"], "reverse_ms": m["rev"],
+            "checkpoint_every": m["st"]["checkpoint_every"], "checkpoint_bytes": m["st"]["checkpoint_bytes"],
+            "reconstruction_error": m["st"]["reconstruction_error"], "target": "<= 3", "clocks": m["clocks"]}
+
+
+def main_batched_adjoint(args, tp, torch, rank, world, local, dist):
+    w = batched_workload(args, rank, time_dependent=True)
+    m = batched_adjoint_measure(w, tp, torch, local, args.steps, max(1, min(args.warmup, 2)))
+    st = m["st"]
     if rank == 0:
-        line = {"metric": "adjoint/forward time ratio", "value": a / f, "unit": "x", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": a, "higher_is_better": False,
+        line = {"metric": "adjoint/forward time ratio", "value": m["a"] / m["f"], "unit": "x", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["a"], "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (seeded Philox variants and beams)",
-                "config": {"workload": w["name"], "turns_per_step": turns,
-                           "parameters": int(sum(len(p) for p in params))},
-                "detail": {"batched_forward_ms": f, "batched_adjoint_ms": a, "reverse_ms": float(np.median(rev)),
+                "config": {"workload": w["name"], "turns_per_step": w["turns"], "parameters": m["params"]},
+                "detail": {"batched_forward_ms": m["f"], "batched_adjoint_ms": m["a"], "reverse_ms": m["rev"],
                            "checkpoint_every": st["checkpoint_every"], "checkpoint_bytes": st["checkpoint_bytes"],
                            "reconstruction_error": st["reconstruction_error"],
-                           "forward_rate": st["units"] / (f * 1e-3), "target": "<= 3"},
-                "gpu_launches": 3 * args.steps, "clocks": clk}
+                           "forward_rate": st["units"] / (m["f"] * 1e-3), "target": "<= 3"},
+                "gpu_launches": 3 * args.steps, "clocks": m["clocks"]}
         print(json.dumps(line))
 
 

@@ -50,3 +50,10 @@ def col_rel_err(a, ref):
     scale = np.abs(ref).max(axis=0)
     scale = np.where(scale > 0, scale, 1.0)
     return float((np.abs(a - ref).max(axis=0) / scale).max())
+
+
+def golden_lattice(case):
+    """The Lattice of a golden case: its element records and misalignment rows."""
+    rows = [{k: [float.fromhex(v) for v in row[k]] for k in ("t1", "t2", "r1", "r2")}
+            for row in case.get("misalign", [])]
+    return tp.Lattice.from_records(case["elements"], misalign=rows)

@@ -614,8 +614,49 @@ def body(r, h, L, beti):  # exact_bend_body, tracking.jl:858-894
     return (xn, pxn, y + py * das, py, z + dp1 * das - L * beti, d)
 
 
-def apply_pass(e, r, beti):
-    """pass!(elem, r, beti) for every supported element kind."""
+# Kinds whose pass! starts with apply_misalignment(r, elem.t1) (and `elem.r1 * r`
+# when r1 is not all zero) and ends with `elem.r2 * r` and apply_misalignment(r,
+# elem.t2): tracking.jl:115-132, 386-427, 438-459, 470-491, 529-570, 579-607,
+# 616-633, 657-706, 901-973, 981-1060, 1152-1170, 1509-1525.
+MISALIGNED_KINDS = {"DRIFT", "QUADRUPOLE", "SEXTUPOLE", "OCTUPOLE", "SOLENOID", "CORRECTOR", "THIN_MULTIPOLE",
+                    "SBEND", "EXACT_SBEND", "DRIFT_SC", "QUADRUPOLE_SC", "SEXTUPOLE_SC", "OCTUPOLE_SC", "SBEND_SC",
+                    "LBEND", "WIGGLER"}
+
+
+def add_t(r, t):  # apply_misalignment(r, t) = r + t, tracking.jl:64-66
+    return tuple(r[i] + t[i] for i in range(6))
+
+
+def mat_vec(R, r):
+    """SMatrix{6,6} * SVector{6}: R stored column-major (R[i + 6 j] is row i,
+    column j); each row summed over the columns left to right."""
+    out = []
+    for i in range(6):
+        acc = R[i] * r[0]
+        for j in range(1, 6):
+            acc = acc + R[i + 6 * j] * r[j]
+        out.append(acc)
+    return tuple(out)
+
+
+def apply_pass(e, r, beti, mis=None):
+    """pass!(elem, r, beti): misalignment (when the element has a row) around the map."""
+    row = mis[e["misalign_index"]] if (mis and e.get("misalign_index", -1) >= 0) else None
+    if row is None or e["kind"] not in MISALIGNED_KINDS:
+        return apply_map(e, r, beti)
+    r = add_t(r, row["t1"])
+    if any(v != 0.0 for v in row["r1"]):
+        r = mat_vec(row["r1"], r)
+    if e["kind"] in ("SBEND_SC", "LBEND") and e["L"] == 0.0:
+        return nan6()
+    r = apply_map(e, r, beti)
+    if any(v != 0.0 for v in row["r2"]):
+        r = mat_vec(row["r2"], r)
+    return add_t(r, row["t2"])
+
+
+def apply_map(e, r, beti):
+    """The map of pass!(elem, r, beti) between the misalignments, for every supported element kind."""
     kind = e["kind"]
     if kind in ("MARKER", "SPACE_CHARGE"):
         return r
@@ -820,8 +861,9 @@ def apply_pass(e, r, beti):
     raise ValueError(kind)
 
 
-def ringpass(elems, parts, beti, nturns=1, aperture=(0.0, 0.0)):
-    """ringpass!/linepass! (lattice.jl:260-317) on a list of particles."""
+def ringpass(elems, parts, beti, nturns=1, aperture=(0.0, 0.0), misalign=None):
+    """ringpass!/linepass! (lattice.jl:260-317) on a list of particles;
+    `misalign` lists the misalignment rows the elements' misalign_index select."""
     coords = [tuple(p) for p in parts]
     lost = [0] * len(coords)
     lost_turn = [-1] * len(coords)
@@ -832,7 +874,7 @@ def ringpass(elems, parts, beti, nturns=1, aperture=(0.0, 0.0)):
             for i in range(len(coords)):
                 if lost[i] == 1:
                     continue
-                rn = apply_pass(e, coords[i], beti)
+                rn = apply_pass(e, coords[i], beti, misalign)
                 out = lost_check(rn) or (ax > 0.0 and abs(rn[0]) > ax) or (ay > 0.0 and abs(rn[2]) > ay)
                 if out:
                     lost[i], lost_turn[i], lost_elem[i] = 1, t, ie
@@ -845,11 +887,77 @@ def hexify(rows):
     return [[float(v).hex() for v in row] for row in rows]
 
 
-def case(name, elems, parts, energy, nturns=1, aperture=(0.0, 0.0)):
+def case(name, elems, parts, energy, nturns=1, aperture=(0.0, 0.0), misalign=None):
     beti = beti_of(energy)
-    out, lost, lt, le = ringpass(elems, parts, beti, nturns, aperture)
-    return dict(name=name, energy=energy, beti=beti.hex(), nturns=nturns, aperture=list(aperture),
-                elements=elems, input=hexify(parts), output=hexify(out), lost=lost, lost_turn=lt, lost_elem=le)
+    out, lost, lt, le = ringpass(elems, parts, beti, nturns, aperture, misalign)
+    d = dict(name=name, energy=energy, beti=beti.hex(), nturns=nturns, aperture=list(aperture),
+             elements=elems, input=hexify(parts), output=hexify(out), lost=lost, lost_turn=lt, lost_elem=le)
+    if misalign:
+        d["misalign"] = [{k: [float(v).hex() for v in row[k]] for k in ("t1", "t2", "r1", "r2")}
+                         for row in misalign]
+    return d
+
+
+def rot_xy(phi):
+    """Roll about the beam axis by phi: (x, y) and (px, py) rotated alike (column-major 6x6)."""
+    c, sn = math.cos(phi), math.sin(phi)
+    m = [0.0] * 36
+    for i in range(6):
+        m[i + 6 * i] = 1.0
+    for a, b in ((0, 2), (1, 3)):
+        m[a + 6 * a], m[a + 6 * b] = c, sn
+        m[b + 6 * a], m[b + 6 * b] = -sn, c
+    return m
+
+
+def general_matrix(seed):
+    """A non-orthogonal matrix near the identity (column-major), deterministic."""
+    m = [0.0] * 36
+    v = seed
+    for j in range(6):
+        for i in range(6):
+            v = (v * 1103515245 + 12345) % (1 << 31)
+            m[i + 6 * j] = (1.0 if i == j else 0.0) + ((v / (1 << 31)) - 0.5) * 0.02
+    return m
+
+
+def misalignment_cases(energy):
+    """Elements with offsets t1/t2 and rotations r1/r2 (the reference's Drift,
+    Quadrupole, Sextupole, SBend, ExactSBend, ... misalignment fields)."""
+    zero = [0.0] * 36
+    offs = [(1.5e-4, -2.0e-5, -7.0e-5, 1.2e-5, 3.0e-5, 0.0), (-1.5e-4, 2.0e-5, 7.0e-5, -1.2e-5, -3.0e-5, 0.0)]
+    rows = [
+        dict(t1=list(offs[0]), t2=list(offs[1]), r1=rot_xy(2e-3), r2=rot_xy(-2e-3)),   # offset and roll
+        dict(t1=list(offs[0]), t2=list(offs[1]), r1=zero, r2=zero),                     # offset only
+        dict(t1=[0.0] * 6, t2=[0.0] * 6, r1=general_matrix(7), r2=general_matrix(11)),  # general matrices
+        dict(t1=[2e-5, 0.0, -1e-5, 0.0, 0.0, 1e-6], t2=[0.0] * 6, r1=zero, r2=rot_xy(1e-3)),
+    ]
+
+    def mis(e, k):
+        e = dict(e)
+        e["misalign_index"] = k
+        return e
+
+    a = math.pi / 9
+    dba = [Drift(2.0), mis(SBend(1.0, a, a / 2, a / 2), 1), Drift(0.5), mis(Quadrupole(0.4, 1.5), 0), Drift(0.5),
+           mis(Quadrupole(0.4, -1.2), 2), Drift(0.5), mis(Quadrupole(0.4, 1.5), 3), Drift(0.5),
+           mis(SBend(1.0, a, a / 2, a / 2), 0), Drift(2.0)]
+    return [
+        ("MisalignedQuadrupole", [mis(Quadrupole(0.4, 1.3), 0)], rows, 1),
+        ("MisalignedSextupoleGeneral", [mis(Sextupole(0.4, 2.0), 2)], rows, 1),
+        ("MisalignedDriftRotation", [mis(Drift(0.7), 2)], rows, 1),
+        ("MisalignedSBend", [mis(SBend(0.9, 0.15, 0.03, 0.02), 1)], rows, 1),
+        ("MisalignedExactSBend", [mis(ExactSBend(0.9, 0.15, 0.03, 0.02), 0)], rows, 1),
+        ("MisalignedExactSBendGeneral", [mis(ExactSBend(1.5, 2.0 * math.pi / 40.0, math.pi / 40.0,
+                                                        math.pi / 40.0), 2)], rows, 1),
+        ("MisalignedOtherKinds", [mis(ThinMultipole(1.0, [0.0, 0.01, 0.0, 0.0], [1e-4, 0.2, 3.0, 0.0], max_order=2), 0),
+                                  mis(Solenoid(0.5, 0.3), 1), mis(Corrector(0.3, 1e-4, -2e-4), 3),
+                                  mis(QuadrupoleSC(0.4, k1=1.1), 2), mis(SBendSC(0.9, 0.15, 0.03, 0.02), 0),
+                                  mis(DriftSC(0.6), 3), mis(Octupole(0.3, 40.0), 1),
+                                  mis(LBend(0.9, 0.15, 0.03, 0.02, K=0.8), 2),
+                                  mis(Wiggler(0.25, lw=0.05, Bmax=0.8, Nsteps=3, energy=3.5e9), 3)], rows, 1),
+        ("MisalignedDBA_line_3passes", dba, rows, 3),
+    ]
 
 
 def element_cases(energy):
@@ -953,6 +1061,8 @@ def main():
     cases = []
     for name, elems in element_cases(energy) + extra_cases(energy):
         cases.append(case(name, elems, parts, energy))
+    for name, elems, rows, nturns in misalignment_cases(energy):
+        cases.append(case(name, elems, parts, energy, nturns=nturns, misalign=rows))
     cases.append(case("FODO_line", fodo_line(), parts, energy))
     cases.append(case("DBA_line", dba_line(), parts, energy))
     cases.append(case("Bend_pi4", [SBend(1.0, math.pi / 4, math.pi / 8, math.pi / 8)], parts, energy))

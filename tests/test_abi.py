@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle_ref
-from conftest import ROOT, has_gpu, tp
+from conftest import ROOT, golden_lattice, has_gpu, tp
 
 abi = tp._abi
 W = __import__("trackpad_b200.workloads", fromlist=["x"])
@@ -100,20 +100,10 @@ def test_flop_model_matches_oracle_op_count(lat_name, golden):
     elif lat_name == "dba":
         lats = [(W.dba_ring(cells=2), 3e9)]
     else:
-        lats = [(tp.Lattice([]), 3.5e9)]
-        lats = []
         for c in golden["cases"]:
-            arr, aux = abi.elem_array_aux(c["elements"])
-            aux = np.asarray(aux, dtype=np.float64)
-            h = C.c_void_p()
-            assert abi.lib().tp_lattice_create_ex(arr, len(c["elements"]), None, 0,
-                                                  aux.ctypes.data_as(C.c_void_p) if len(aux) else None, len(aux),
-                                                  C.byref(h)) == 0
-            out = np.zeros(len(c["elements"]))
-            abi.lib().tp_lattice_flops(h, out.ctypes.data_as(C.c_void_p))
-            ref, _ = oracle_ref.count_flops(c["elements"], float.fromhex(c["beti"]))
-            assert out.tolist() == ref.tolist(), c["name"]
-            abi.lib().tp_lattice_destroy(h)
+            lat = golden_lattice(c)  # element records and misalignment rows
+            ref, _ = oracle_ref.count_flops(lat, float.fromhex(c["beti"]))
+            assert lat.flops_per_element().tolist() == ref.tolist(), c["name"]
         return
     for lat, e in lats:
         ref, _ = oracle_ref.count_flops(lat, tp.beti(tp.Beam(e)))

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 import oracle_ref
-from conftest import col_rel_err, tp, unhex
+from conftest import col_rel_err, golden_lattice, tp, unhex
 
 pytestmark = pytest.mark.gpu
 W = __import__("trackpad_b200.workloads", fromlist=["x"])
@@ -22,7 +22,7 @@ USES_EXP = set()  # exp now comes from the shared libm too: no exception left
 
 
 def _run_case(c, contract):
-    lat = tp.Lattice.from_records(c["elements"])
+    lat = golden_lattice(c)
     coords = np.asfortranarray(unhex(c["input"]))
     n = coords.shape[0]
     lost = np.zeros(n, np.int64)

@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 import oracle_ref
-from conftest import ROOT, unhex
+from conftest import ROOT, golden_lattice, unhex
 
 
 def _cases(golden):
@@ -25,10 +25,13 @@ def test_fixture_regenerates(golden, tmp_path):
     spec = importlib.util.spec_from_file_location("mg", os.path.join(ROOT, "tests", "golden", "make_golden.py"))
     mg = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(mg)
-    for c in golden["cases"][:8]:
+    mis = [c for c in golden["cases"] if c.get("misalign")]
+    for c in golden["cases"][:8] + mis[:2]:
         inp = unhex(c["input"]).tolist()
+        rows = [{k: [float.fromhex(v) for v in row[k]] for k in ("t1", "t2", "r1", "r2")}
+                for row in c.get("misalign", [])]
         out, lost, lt, le = mg.ringpass(c["elements"], inp, float.fromhex(c["beti"]), c["nturns"],
-                                        tuple(c["aperture"]))
+                                        tuple(c["aperture"]), rows)
         assert [[float(v).hex() for v in r] for r in out] == c["output"]
 
 
@@ -40,7 +43,7 @@ def test_oracle_matches_golden_bitwise(golden):
         lt = np.full(coords.shape[0], -1, dtype=np.int32)
         le = np.full(coords.shape[0], -1, dtype=np.int32)
         beti = float.fromhex(c["beti"])
-        oracle_ref.ringpass(c["elements"], coords, lost, beti, c["nturns"], aperture=tuple(c["aperture"]),
+        oracle_ref.ringpass(golden_lattice(c), coords, lost, beti, c["nturns"], aperture=tuple(c["aperture"]),
                             lost_turn=lt, lost_elem=le)
         ref = unhex(c["output"])
         same = (coords == ref) | (np.isnan(coords) & np.isnan(ref))
@@ -67,3 +70,17 @@ def test_loss_cases_have_losses(golden):
         c = by[name]
         assert 0 < sum(c["lost"]) < len(c["lost"])
     assert max(by["FODO_sext_losses"]["lost_turn"]) > 0
+
+
+def test_golden_has_misalignment_cases(golden):
+    """Offsets (t1, t2), rolls and general non-orthogonal r1/r2 matrices, on
+    single elements and on the DBA line over several passes."""
+    mis = [c for c in golden["cases"] if c.get("misalign")]
+    assert len(mis) >= 6
+    rows = mis[0]["misalign"]
+    assert any(float.fromhex(v) != 0.0 for r in rows for v in r["t1"])
+    assert any(float.fromhex(v) != 0.0 for r in rows for v in r["t2"])
+    general = [r for r in rows if any(float.fromhex(v) != 0.0 for v in r["r1"])]
+    assert general
+    by = {c["name"]: c for c in mis}
+    assert by["MisalignedDBA_line_3passes"]["nturns"] == 3

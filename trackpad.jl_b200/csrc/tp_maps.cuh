@@ -105,34 +105,7 @@ __device__ __forceinline__ void bend_kick(P6& s, const double* pa, const double*
     s.z = s.z + Kh * s.x * beti;
 }
 
-// drift6 (exact branch) with its NormL = L/sqrt(pz2) returned through `NormL`
-// (NaN when pz2 <= 0, where the state becomes NaN).
-__device__ __forceinline__ void drift_exact_norm(P6& s, double L, double Lbeti, const DCache& c, double& NormL) {
-    double pz2 = c.A - s.px * s.px - s.py * s.py;
-    if (pz2 <= 0.0) {
-        set_nan(s);
-        NormL = CUDART_NAN;
-        return;
-    }
-    NormL = L / sqrt(pz2);
-    s.x = s.x + NormL * s.px;
-    s.y = s.y + NormL * s.py;
-    s.z = s.z + NormL * c.bd - Lbeti;
-}
-
-// A second drift6 of the same length right after one (no kick between): px,
-// py and delta are unchanged, so pz2 and NormL = L/sqrt(pz2) are the previous
-// drift's bit for bit and only the position updates remain.  After a NaN drift
-// the state is NaN and stays NaN either way.
-__device__ __forceinline__ void drift_exact_again(P6& s, double NormL, double Lbeti, const DCache& c) {
-    s.x = s.x + NormL * s.px;
-    s.y = s.y + NormL * s.py;
-    s.z = s.z + NormL * c.bd - Lbeti;
-}
-
-// symplectic4_pass (src/tracking.jl:317-341) for one multipole record.  The
-// last drift D(L1) of a Yoshida step and the first D(L1) of the next follow
-// each other with no kick between, so the second reuses the first's NormL.
+// symplectic4_pass (src/tracking.jl:317-341) for one multipole record.
 template <int M, bool EXACT>
 __device__ __noinline__ void multipole(P6& s, const double* w, int nsteps, double beti) {
     const double L1 = w[mp::L1], L2 = w[mp::L2], K1 = w[mp::K1], K2 = w[mp::K2];
@@ -143,16 +116,29 @@ __device__ __noinline__ void multipole(P6& s, const double* w, int nsteps, doubl
     DCache c;
     make_cache(s, beti, c);
     // D(L1) K(K1) D(L2) K(K2) D(L2) K(K1) D(L1) per step, as one loop (code size).
-    double carry = 0.0;
+    // The last D(L1) of a step and the first D(L1) of the next follow each
+    // other with no kick between: px, py and delta are unchanged, so the second
+    // reuses the first's NormL = L1/sqrt(pz2) (the same bits).  Where pz2 <= 0
+    // drift6 returns NaN coordinates; here NormL is NaN, which makes x, y and z
+    // NaN (px and py follow in the next kick): x is NaN either way, so
+    // check_lost flags the particle at this element and its entrance
+    // coordinates are kept, as with drift6's NaN vector.
+    double NormL = 0.0;
 #pragma unroll 1
     for (int k = 0; k < 4 * nsteps; ++k) {
         const int j = k & 3;
         const bool outer = (j == 0) || (j == 3);
+        const double Lk = outer ? L1 : L2;
         if (EXACT) {
-            if (j == 0 && k > 0) drift_exact_again(s, carry, L1b, c);
-            else drift_exact_norm(s, outer ? L1 : L2, outer ? L1b : L2b, c, carry);
+            if (j != 0 || k == 0) {
+                double pz2 = c.A - s.px * s.px - s.py * s.py;
+                NormL = pz2 <= 0.0 ? CUDART_NAN : Lk / sqrt(pz2);
+            }
+            s.x = s.x + NormL * s.px;
+            s.y = s.y + NormL * s.py;
+            s.z = s.z + NormL * c.bd - (outer ? L1b : L2b);
         } else {
-            drift<EXACT>(s, outer ? L1 : L2, outer ? L1b : L2b, c);
+            drift<EXACT>(s, Lk, outer ? L1b : L2b, c);
         }
         if (j != 3) thin_kick<M>(s, pa, pb, j == 1 ? K2 : K1);
     }
@@ -194,19 +180,14 @@ __device__ __noinline__ void sbend(P6& s, const double* w, const RecHdr& h, doub
     const double K1h = K1 * irho, K2h = K2 * irho;
     DCache c;
     make_cache(s, beti, c);
-    // As in multipole(): a step's first D(L1) reuses the previous step's last.
-    double carry = 0.0;
     for (int st = 0; st < h.nsteps; ++st) {
-        if (!EXACT) drift<EXACT>(s, L1, L1b, c);
-        else if (st > 0) drift_exact_again(s, carry, L1b, c);
-        else drift_exact_norm(s, L1, L1b, c, carry);
+        drift<EXACT>(s, L1, L1b, c);
         bend_kick<M>(s, pa, pb, K1, K1h, irho, beti);
         drift<EXACT>(s, L2, L2b, c);
         bend_kick<M>(s, pa, pb, K2, K2h, irho, beti);
         drift<EXACT>(s, L2, L2b, c);
         bend_kick<M>(s, pa, pb, K1, K1h, irho, beti);
-        if (EXACT) drift_exact_norm(s, L1, L1b, c, carry);
-        else drift<EXACT>(s, L1, L1b, c);
+        drift<EXACT>(s, L1, L1b, c);
     }
     if (h.flags & RF_FRINGE_OUT)
         edge_fringe(s, irho, w[sb::FX_OUT], w[sb::E_OUT], w[sb::FC_OUT], h.method_out, h.flags & RF_FC_OUT_ZERO, true);
@@ -215,6 +196,10 @@ __device__ __noinline__ void sbend(P6& s, const double* w, const RecHdr& h, doub
 // ---------------------------------------------------------------------------
 // Exact sector bend (src/tracking.jl:717-973).  dp1 = beti + delta = c.bd.
 // ---------------------------------------------------------------------------
+// One out-of-line copy of asin for the bend maps: a smaller hot loop (the
+// kernels are limited by instruction fetch as much as by the FP64 pipe).
+static __device__ __noinline__ double asin_ool(double x) { return libm::asin(x); }
+
 // pxyz (:717-720) with dp1^2 precomputed.
 __device__ __forceinline__ double pxyz(double dp1sq, double px, double py) {
     double val = dp1sq - px * px - py * py;
@@ -299,7 +284,7 @@ static __device__ __noinline__ void bend_edge(P6& r, double rhoinv, double c, do
     double px_new = r.px * c + (pz - rhoinv * r.x) * s;
     double val1 = jclamp(r.px / d2);
     double val2 = jclamp(px_new / d2);
-    double dasin = libm::asin(val1) - libm::asin(val2);
+    double dasin = asin_ool(val1) - asin_ool(val2);
     double num = r.x * (r.px * s2 + s * s * (2.0 * pz - rhoinv * r.x));
     double den = pxyz(dp1sq, px_new, r.py) + pz * c - r.px * s;
     double x_new = r.x * c + num / den;
@@ -372,7 +357,7 @@ __device__ __forceinline__ void body_carry_init(const P6& r, double dp1, BodyCar
     b.rcp_d2 = is_normal(b.d2) && is_normal(b.d2inv);
     double v = b.dp1sq - r.px * r.px - b.pysq;
     b.pz = v > 0.0 ? sqrt(v) : 0.0;
-    b.as1 = libm::asin(jclamp(r.px / b.d2));
+    b.as1 = asin_ool(jclamp(r.px / b.d2));
 }
 
 // One exact_bend_body call (:869-893) with the carried values.  The three
@@ -385,7 +370,7 @@ __device__ __forceinline__ void body_carry_step(P6& r, BodyCarry& b, double irho
     double pzmx = b.pz - (1.0 + r.x * irho);
     double px_new = r.px * cs + pzmx * sn;
     double q2 = b.rcp_d2 ? div_rcp(px_new, b.d2, b.d2inv) : px_new / b.d2;
-    double as2 = libm::asin(jclamp(q2));
+    double as2 = asin_ool(jclamp(q2));
     double das = b.as1 - as2;
     double dasin = L + (RCP_IRHO ? div_rcp(das, irho, irho_inv) : das / irho);
     double v = b.dp1sq - px_new * px_new - b.pysq;

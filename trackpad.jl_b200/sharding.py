@@ -10,6 +10,8 @@ all-reduce of (3 + number of parameters) doubles per gradient.
   particle_shard(n, rank, world)      contiguous [start, stop) of rank's particles
   variant_shard(costs, world)         variants per rank, balanced by cost (longest first)
   combine_adjoint(terms, all_reduce)  global loss and gradient from per-rank terms
+  distributed_ringpass_(...)          ringpass! of one coordinate matrix split over the ranks,
+                                      each rank tracking its shard, the results gathered back
   distributed_ringpass_adjoint(...)   the adjoint on this rank's shard, combined over the group
 
 Launch one process per GPU (torchrun); the collective runs on whatever
@@ -97,3 +99,87 @@ def distributed_ringpass_adjoint(coords0, lat, beam, lost0, nturns, params, *, s
     st = tracking.last_stats()
     terms = local_terms(loss, grad, st["survivors"], st["particles"], lost_weight)
     return combine_adjoint(terms, torch_all_reduce(group, device), lost_weight)
+
+
+def torch_all_gather(group=None, device=None):
+    """Gather one numpy array per rank (same dtype and trailing shape, leading
+    sizes may differ) over a torch.distributed group: every rank gets the
+    list of all ranks' arrays in rank order.  Arrays are padded to the largest
+    leading size for the collective (all_gather wants equal sizes)."""
+    import torch
+    import torch.distributed as dist
+
+    def gather(a):
+        a = np.ascontiguousarray(a)
+        world = dist.get_world_size(group)
+        n = torch.tensor([a.shape[0]], dtype=torch.int64, device=device)
+        sizes = [torch.zeros_like(n) for _ in range(world)]
+        dist.all_gather(sizes, n, group=group)
+        sizes = [int(x.item()) for x in sizes]
+        m = max(sizes) if sizes else 0
+        buf = np.zeros((m,) + a.shape[1:], dtype=a.dtype)
+        buf[:a.shape[0]] = a
+        t = torch.from_numpy(buf)
+        if device is not None:
+            t = t.to(device)
+        outs = [torch.empty_like(t) for _ in range(world)]
+        dist.all_gather(outs, t, group=group)
+        return [o.cpu().numpy()[:k] for o, k in zip(outs, sizes)]
+
+    return gather
+
+
+def shard_and_gather(coords, lost_flags, rank, world, track_shard, gather, lost_turn=None, lost_elem=None):
+    """Split the N x 6 host matrix `coords` (and its per-particle arrays) into
+    `world` contiguous particle shards, let `track_shard(c, lost, lt, le)`
+    update this rank's shard in place (c is an (n_r, 6) column-major copy),
+    then gather every rank's shard back into the full arrays, in place, on
+    every rank.  Returns this rank's (start, stop)."""
+    n = coords.shape[0]
+    lo, hi = particle_shard(n, rank, world)
+    c = np.asfortranarray(coords[lo:hi])
+    lf = np.ascontiguousarray(lost_flags[lo:hi])
+    lt = None if lost_turn is None else np.ascontiguousarray(lost_turn[lo:hi])
+    le = None if lost_elem is None else np.ascontiguousarray(lost_elem[lo:hi])
+    track_shard(c, lf, lt, le)
+    # one gather of a packed row per particle: 6 coordinates, flag, turn, element
+    packed = np.empty((hi - lo, 9), dtype=np.float64)
+    packed[:, :6] = c
+    packed[:, 6] = lf
+    packed[:, 7] = -1 if lt is None else lt
+    packed[:, 8] = -1 if le is None else le
+    parts = gather(packed)
+    full = np.concatenate(parts, axis=0) if parts else packed
+    if full.shape[0] != n:
+        raise RuntimeError(f"gathered {full.shape[0]} particles, expected {n}")
+    coords[...] = full[:, :6]
+    lost_flags[...] = full[:, 6].astype(np.int64)
+    if lost_turn is not None:
+        lost_turn[...] = full[:, 7].astype(np.int32)
+    if lost_elem is not None:
+        lost_elem[...] = full[:, 8].astype(np.int32)
+    return lo, hi
+
+
+def distributed_ringpass_(coords, lat, beam, lost_flags, nturns, *, group=None, device=None, lost_turn=None,
+                          lost_elem=None, **kw):
+    """ringpass!(coords, lat, beam, lost_flags, nturns) with the particles
+    split over the ranks of `group`: every rank passes the same N x 6 host
+    matrix, tracks its contiguous shard (`particle_shard`) on its own GPU (the
+    current device), and the shards are gathered back so that every rank ends
+    with the whole result, as a single-process call would give.  No collective
+    runs on the tracking path; the gather is one all-gather of 9 doubles per
+    particle (coordinates, flag, turn and element of loss), on `device` when
+    the group's backend is NCCL.  Keywords are those of tracking.ringpass_."""
+    import torch.distributed as dist
+
+    from . import tracking
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    coll_dev = device if dist.get_backend(group) == "nccl" else None
+
+    def track(c, lf, lt, le):
+        if c.shape[0]:
+            tracking.ringpass_(c, lat, beam, lf, nturns, lost_turn=lt, lost_elem=le, **kw)
+
+    return shard_and_gather(coords, lost_flags, rank, world, track, torch_all_gather(group, coll_dev),
+                            lost_turn=lost_turn, lost_elem=lost_elem)

@@ -173,10 +173,14 @@ class Lattice:
         self._sched_key = None
 
     @classmethod
-    def from_records(cls, records, name="LATTICE"):
-        """A lattice from raw C-ABI records (dicts with tp_elem field names, or TpElem)."""
+    def from_records(cls, records, name="LATTICE", misalign=None):
+        """A lattice from raw C-ABI records (dicts with tp_elem field names, or
+        TpElem).  `misalign` lists the misalignment rows (dicts of t1, t2: 6
+        values; r1, r2: 36 values, column-major) that the records'
+        misalign_index select."""
         lat = cls([], name=name)
         lat._records = list(records)
+        lat._mis_rows = list(misalign or [])
         return lat
 
     def __len__(self):
@@ -202,7 +206,15 @@ class Lattice:
         """(tp_elem array, n, misalignment array, nmis, aux float64 array)."""
         if getattr(self, "_records", None) is not None:
             arr, aux = _abi.elem_array_aux(self._records)
-            return arr, len(self._records), (_abi.TpMisalign * 1)(), 0, np.asarray(aux, dtype=np.float64)
+            rows = getattr(self, "_mis_rows", [])
+            marr = (_abi.TpMisalign * max(len(rows), 1))()
+            for k, row in enumerate(rows):
+                for f, n in (("t1", 6), ("t2", 6), ("r1", 36), ("r2", 36)):
+                    vals = [float(v) for v in row[f]]
+                    if len(vals) != n:
+                        raise ValueError(f"misalignment row {k}: {f} needs {n} values")
+                    getattr(marr[k], f)[:] = vals
+            return arr, len(self._records), marr, len(rows), np.asarray(aux, dtype=np.float64)
         elems = self._static_elements()
         arr = (_abi.TpElem * max(len(elems), 1))()
         mis = []
