@@ -54,7 +54,7 @@ def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=10)
-    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--workload", default="dba", choices=["dba", "fodo", "batched", "adjoint", "batched_adjoint",
                                                          "tpsa"])
@@ -237,7 +237,7 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # Adjoint / forward ratio on the gradient workload
 # ---------------------------------------------------------------------------
-def adjoint_ratio(tp, local, turns=256, n=65536, warmup=1, steps=1):
+def adjoint_ratio(tp, local, turns=256, n=65536, warmup=4, steps=1):
     """Loss and gradient with respect to the 120 quadrupole k1 and 80 sextupole
     k2 of the DBA ring, 65,536 Gaussian particles, `turns` turns, against
     ringpass! of the same beam; device times from the library's CUDA events."""
@@ -271,6 +271,7 @@ def adjoint_ratio(tp, local, turns=256, n=65536, warmup=1, steps=1):
                       f"(x^2+y^2)/sigma^2 + 1e3 lost fraction, sigma = 1e-4 m",
             "forward_ms": f, "adjoint_ms": a, "adjoint_forward_pass_ms": a - float(np.median(rev)),
             "adjoint_reverse_ms": float(np.median(rev)), "checkpoint_every": st["checkpoint_every"],
+            "checkpoint_every_source": {0: "given", 1: "autotuner trial", 2: "autotuned by timing"}[st["k_tuning"]],
             "checkpoint_bytes": st["checkpoint_bytes"], "reconstruction_error": st["reconstruction_error"],
             "loss": loss, "target": "<= 3"}
 
@@ -479,13 +480,13 @@ def batched_summary(args, tp, torch, local):
     """The batched forward workload (256 DBA variants, 100-turn steps) as an
     object of the default line."""
     w = batched_workload(argparse.Namespace(nvar=0, turns=0), 0)
-    m = batched_measure(w, tp, torch, local, steps=3, warmup=3)
+    m = batched_measure(w, tp, torch, local, steps=3, warmup=5)
     peak = tp.probe_fp64_peak(local)
     achieved = (m["flops"] / 3) / (m["kernel_ms"] * 1e-3) / 1e12
     value = m["units"] / m["elapsed"]
     lbl = lattice_by_lattice(w, m, tp, torch, local)
     return {"metric": "particle*element*turns/s FP64 (batched)", "value": value, "unit": "particle*element*turns/s",
-            "steps": 3, "warmup": 3, "ms_per_step": m["elapsed"] / 3 * 1e3,
+            "steps": 3, "warmup": 5, "ms_per_step": m["elapsed"] / 3 * 1e3,
             "config": {"workload": w["name"], "turns_per_step": w["turns"],
                        "particles": int(w["coords"].shape[0]),
                        "schedule": {1: "static tiles", 2: "pooled refill"}.get(m["st"]["schedule"]),
@@ -567,7 +568,7 @@ def main_adjoint(args, tp, torch, rank, world, local, dist):
     import trackpad_b200.workloads as W
     turns = args.turns or 256
     clocks = Clocks(local)
-    r = adjoint_ratio(tp, local, turns=turns, warmup=max(1, min(args.warmup, 2)), steps=args.steps)
+    r = adjoint_ratio(tp, local, turns=turns, warmup=max(4, args.warmup), steps=args.steps)
     clk = clocks.stop()
     # end to end through the public API with host arrays (inputs staged every call)
     lat, beam = W.dba_ring(), W.dba_beam()
@@ -632,9 +633,9 @@ def batched_adjoint_summary(args, tp, torch, local):
     variants, 16,384 particles each, 50-turn steps) as an object of the
     default line."""
     w = batched_workload(argparse.Namespace(nvar=0, turns=0), 0, time_dependent=True)
-    m = batched_adjoint_measure(w, tp, torch, local, steps=2, warmup=1)
+    m = batched_adjoint_measure(w, tp, torch, local, steps=2, warmup=4)
     return {"metric": "batched adjoint/forward time ratio", "value": m["a"] / m["f"], "unit": "x",
-            "higher_is_better": False, "steps": 2, "warmup": 1,
+            "higher_is_better": False, "steps": 2, "warmup": 4,
             "config": {"workload": w["name"], "turns_per_step": w["turns"], "parameters": m["params"]},
             "batched_forward_ms": m["f"], "batched_adjoint_ms": m["a"], "reverse_ms": m["rev"],
             "checkpoint_every": m["st"]["checkpoint_every"], "checkpoint_bytes": m["st"]["checkpoint_bytes"],
@@ -643,7 +644,7 @@ def batched_adjoint_summary(args, tp, torch, local):
 
 def main_batched_adjoint(args, tp, torch, rank, world, local, dist):
     w = batched_workload(args, rank, time_dependent=True)
-    m = batched_adjoint_measure(w, tp, torch, local, args.steps, max(1, min(args.warmup, 2)))
+    m = batched_adjoint_measure(w, tp, torch, local, args.steps, max(4, args.warmup))
     st = m["st"]
     if rank == 0:
         line = {"metric": "adjoint/forward time ratio", "value": m["a"] / m["f"], "unit": "x", "n_gpus": world,

@@ -181,12 +181,21 @@ typedef struct tp_opts {
                                   the reference's operations in its order (exact
                                   bends amplify a changed rounding to ~1e-11)     */
     int32_t block_size;        /* threads per block; 0 = autotuned                */
-    int32_t ppt;               /* particles per thread (1 or 2); 0 = autotuned    */
-    int32_t schedule;          /* 0 = autotuned: the first two multi-turn calls of a
-                                  configuration run static and lane refill, later
-                                  calls the faster (all give identical results);
-                                  1 = static, 2 = lane refill (batched: lanes of a
-                                  variant refill from that variant's particles)   */
+    int32_t min_blocks;        /* tracking kernel instance: registers sized for 7,
+                                  6 or 5 resident 128-thread blocks per SM (more
+                                  blocks hide more latency, fewer spill less);
+                                  0 = autotuned.  The build with FMA contraction
+                                  and tables with kinds outside the integrator
+                                  core have the 7-block instance only             */
+    int32_t schedule;          /* 0 = autotuned; 1 = static, 2 = lane refill
+                                  (batched: lanes of a variant refill from that
+                                  variant's particles).  Autotuning (schedule and
+                                  min_blocks 0): the first multi-turn calls of a
+                                  configuration run static and lane refill at 7
+                                  blocks, then 6 and 5 blocks with the faster
+                                  schedule, each timed on the call's own work;
+                                  later calls keep the fastest.  Every choice
+                                  gives identical results                         */
     int32_t table_in_smem;     /* 1: stage the element table into shared memory by a
                                   bulk (TMA) copy at the start of each block; default
                                   0: read it through the L1 cache.  On the DBA ring the
@@ -212,7 +221,7 @@ typedef struct tp_stats {
     int64_t h2d_bytes;
     int64_t d2h_bytes;
     int32_t block_size;
-    int32_t ppt;
+    int32_t min_blocks;        /* resident blocks per SM of the kernel instance   */
     int32_t grid;
     int32_t launches;          /* kernels this library launched in the call      */
     int32_t schedule;          /* 1 = static, 2 = lane refill                      */
@@ -396,7 +405,12 @@ typedef struct tp_adjoint_stats {
     double reverse_ms;            /* device time of the reverse sweep             */
     double reconstruction_error;
     int32_t launches;
-    int32_t reserved;
+    int32_t k_tuning;             /* 0: K given by the caller (or a loss-only call,
+                                     where K does not matter); 1: the call was a
+                                     timing trial of the K autotuner; 2: K is the
+                                     autotuner's choice                          */
+    double tuned_ms;              /* forward + reverse device time of the chosen K
+                                     in its trial (0 until the trials are done)  */
 } tp_adjoint_stats;
 TP_API int tp_last_adjoint_stats(tp_adjoint_stats* out);
 

@@ -95,6 +95,28 @@ def test_checkpoint_interval_changes_nothing_but_memory():
             assert np.abs(g - ref[1]).max() <= 1e-10 * np.abs(ref[1]).max()
 
 
+def test_checkpoint_interval_autotuner_trials_then_settles():
+    """checkpoint_every = 0: the first gradient calls of a configuration each
+    time one candidate K (1, 2, 4, 8), later calls keep the fastest whose
+    reconstruction error stayed small; tuned and fixed-K gradients agree within
+    1e-10 of the largest component."""
+    lat, beam = W.dba_ring(cells=2), W.dba_beam()
+    params = W.magnet_indices(lat)
+    c0 = W.gaussian(160, seed=23)
+    _, gref = tp.ringpass_adjoint(c0, lat, beam, None, 12, params, sigma=SIGMA, aperture=0.02, checkpoint_every=1)
+    assert tp.adjoint_stats()["k_tuning"] == 0
+    ks, states = [], []
+    for _ in range(6):
+        _, g = tp.ringpass_adjoint(c0, lat, beam, None, 12, params, sigma=SIGMA, aperture=0.02, checkpoint_every=0)
+        st = tp.adjoint_stats()
+        ks.append(st["checkpoint_every"])
+        states.append(st["k_tuning"])
+        assert np.abs(g - gref).max() <= 1e-10 * np.abs(gref).max()
+    assert ks[:4] == [1, 2, 4, 8] and states[:4] == [1, 1, 1, 1]
+    assert states[4:] == [2, 2] and ks[4] == ks[5] and ks[4] in (1, 2, 4, 8)
+    assert tp.adjoint_stats()["tuned_ms"] > 0
+
+
 def test_adjoint_with_losses():
     """Dynamic-aperture grid particles: some are lost, and the gradient is taken
     over the oracle's survivor set."""

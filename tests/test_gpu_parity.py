@@ -319,21 +319,55 @@ def test_batched_schedules_with_losses_equal_lattice_by_lattice(schedule):
         assert np.array_equal(lt[s], rlt) and np.array_equal(le[s], rle)
 
 
-def test_autotuned_schedule_settles_and_keeps_results():
-    """schedule=0: the first two multi-turn calls try static and refill, later
-    calls keep one of them; every call gives the same bits."""
+def test_autotuned_launch_settles_and_keeps_results():
+    """schedule = min_blocks = 0: the first multi-turn calls try static and
+    refill at 7 resident blocks per SM, then 6 and 5 blocks with the faster
+    schedule; later calls keep the fastest; every call gives the same bits."""
     lat, beam = W.dba_ring(cells=2), W.dba_beam()
     c0 = np.asfortranarray(np.concatenate([W.gaussian(300, seed=70), W.da_grid(16, 16)]))
     seen, outs = [], []
-    for _ in range(4):
+    for _ in range(7):
         c = c0.copy(order="F")
         l = np.zeros(len(c), np.int64)
         tp.ringpass_(c, lat, beam, l, 6, aperture=0.02)
-        seen.append(tp.last_stats()["schedule"])
+        st = tp.last_stats()
+        seen.append((st["schedule"], st["min_blocks"]))
         outs.append((c, l))
-    assert seen[:2] == [1, 2] and seen[2] == seen[3] and seen[2] in (1, 2)
+    assert seen[0] == (1, 7) and seen[1] == (2, 7)
+    assert [m for _, m in seen[2:4]] == [6, 5] and seen[2][0] == seen[3][0]
+    assert seen[4] == seen[5] == seen[6] and seen[4] in seen[:4]
     for c, l in outs[1:]:
         assert np.array_equal(c, outs[0][0]) and np.array_equal(l, outs[0][1])
+
+
+@pytest.mark.parametrize("minb", [5, 6, 7])
+def test_every_occupancy_instance_gives_the_same_bits(minb):
+    """The kernel instances sized for 5, 6 and 7 resident blocks per SM, single
+    lattice and batched, bit-identical to the oracle / to each other."""
+    lat, beam = W.dba_ring(cells=3), W.dba_beam()
+    c0 = np.asfortranarray(np.concatenate([W.gaussian(500, seed=71), W.da_grid(12, 12)]))
+    c = c0.copy(order="F")
+    l = np.zeros(len(c), np.int64)
+    tp.ringpass_(c, lat, beam, l, 5, aperture=0.02, schedule=2, min_blocks=minb)
+    assert tp.last_stats()["min_blocks"] == minb
+    r = c0.copy(order="F")
+    rl = np.zeros(len(r), np.int64)
+    oracle_ref.ringpass(lat, r, rl, tp.beti(beam), 5, aperture=(0.02, 0.02))
+    assert np.array_equal(c, r) and np.array_equal(l, rl)
+    variants = W.dba_variants(nvar=3, seed=12, n_base=200, cells_range=(2, 4))
+    counts = [n for _, n in variants]
+    poff = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    coords = np.asfortranarray(np.concatenate([W.gaussian(n, seed=80 + i) for i, n in enumerate(counts)]))
+    batch = tp.Batch([v for v, _ in variants])
+    outs = []
+    for m in (7, minb):
+        cb = coords.copy(order="F")
+        lb = np.zeros(len(cb), np.int64)
+        batch.ringpass_(cb, poff, np.full(3, tp.beti(beam)), lb, 5, aperture=0.02, schedule=2, min_blocks=m,
+                        use_graph=True)
+        assert tp.last_stats()["min_blocks"] == m
+        outs.append((cb, lb))
+    assert np.array_equal(outs[0][0], outs[1][0]) and np.array_equal(outs[0][1], outs[1][1])
 
 
 def test_batched_time_dependent_equals_lattice_by_lattice():

@@ -62,7 +62,7 @@ class TpMisalign(C.Structure):
 class TpOpts(C.Structure):
     _fields_ = [
         ("size", C.c_int32), ("exact_hamiltonian", C.c_int32), ("device_pointers", C.c_int32),
-        ("fp_contract", C.c_int32), ("block_size", C.c_int32), ("ppt", C.c_int32), ("schedule", C.c_int32),
+        ("fp_contract", C.c_int32), ("block_size", C.c_int32), ("min_blocks", C.c_int32), ("schedule", C.c_int32),
         ("table_in_smem", C.c_int32), ("aperture_x", C.c_double), ("aperture_y", C.c_double), ("stream", C.c_void_p),
     ]
 
@@ -71,7 +71,7 @@ class TpStats(C.Structure):
     _fields_ = [
         ("particles", C.c_int64), ("survivors", C.c_int64), ("element_passes", C.c_int64), ("units", C.c_double),
         ("flops", C.c_double), ("kernel_ms", C.c_double), ("total_ms", C.c_double), ("h2d_bytes", C.c_int64),
-        ("d2h_bytes", C.c_int64), ("block_size", C.c_int32), ("ppt", C.c_int32), ("grid", C.c_int32),
+        ("d2h_bytes", C.c_int64), ("block_size", C.c_int32), ("min_blocks", C.c_int32), ("grid", C.c_int32),
         ("launches", C.c_int32), ("schedule", C.c_int32), ("fp_contract", C.c_int32),
     ]
 
@@ -84,7 +84,8 @@ class TpAdjointStats(C.Structure):
     _fields_ = [
         ("checkpoint_every", C.c_int32), ("segments", C.c_int32), ("checkpoint_bytes", C.c_int64),
         ("particles", C.c_int64), ("units", C.c_double), ("forward_ms", C.c_double), ("reverse_ms", C.c_double),
-        ("reconstruction_error", C.c_double), ("launches", C.c_int32), ("reserved", C.c_int32),
+        ("reconstruction_error", C.c_double), ("launches", C.c_int32), ("k_tuning", C.c_int32),
+        ("tuned_ms", C.c_double),
     ]
 
 

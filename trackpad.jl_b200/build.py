@@ -42,7 +42,7 @@ def build(verbose=False, ptxas_info=False):
         base += ["-Xptxas", "-v"]
     units = [
         ("tp_track_fast.o", "tp_track.cu", ["-DTP_NS=fast", "-fmad=true"]),
-        ("tp_track_strict.o", "tp_track.cu", ["-DTP_NS=strict", "-fmad=false"]),
+        ("tp_track_strict.o", "tp_track.cu", ["-DTP_NS=strict", "-fmad=false", "-DTP_OCC_VARIANTS"]),
         ("tp_runtime.o", "tp_runtime.cu", ["-fmad=false"]),
         ("tp_adjoint.o", "tp_adjoint.cu", ["-fmad=false"]),
         ("tp_compile.o", "tp_compile.cpp", ["-fmad=false", "-x", "cu"]),

@@ -35,6 +35,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <mutex>
 #include <vector>
 
 #include "tp_internal.h"
@@ -579,6 +580,80 @@ int32_t auto_interval(int64_t ntot, int32_t nturns) {
     return std::max(nturns, 1);
 }
 
+// Time-based choice of K (checkpoint_every = 0).  The reverse sweep rebuilds
+// each segment with the maps' exact time-reversed forms, so K trades
+// checkpoint memory and traffic against reconstruction drift, not compute.
+// The first gradient calls of a configuration (particles, turns, variants,
+// table, parameters, drift) each run one candidate K in {1, 2, 4, 8} whose
+// checkpoints fit the memory budget, timed on the caller's own work (forward +
+// reverse device time); later calls keep the fastest candidate whose
+// reconstruction error stayed within kRecTol (else the smallest K).
+constexpr double kRecTol = 1e-10;
+struct KTune {
+    uint64_t key = 0;
+    int32_t cand[4] = {};
+    float ms[4] = {};
+    double rec[4] = {};
+    int ncand = 0, ntried = 0;
+    int32_t best = 1;
+    float best_ms = 0.f;
+};
+std::mutex g_ktune_mu;
+KTune g_ktune[16];
+
+uint64_t ktune_key(std::initializer_list<int64_t> parts) {
+    uint64_t h = 1469598103934665603ull;
+    for (int64_t v : parts)
+        for (int k = 0; k < 8; ++k) {
+            h ^= uint64_t(v >> (8 * k)) & 0xffu;
+            h *= 1099511628211ull;
+        }
+    return h | 1ull;
+}
+
+// K for this call and whether it is a timing trial (*state: 1 trial, 2 settled).
+int32_t ktune_pick(int device, uint64_t key, int64_t ntot, int32_t nturns, int* state) {
+    std::lock_guard<std::mutex> g(g_ktune_mu);
+    KTune& t = g_ktune[device & 15];
+    if (t.key != key) {
+        t = KTune{};
+        t.key = key;
+        const int32_t kmin = auto_interval(ntot, nturns);  // smallest K that fits the budget
+        for (int32_t K : {1, 2, 4, 8})
+            if (K >= kmin && K <= std::max(nturns, 1) && t.ncand < 4) t.cand[t.ncand++] = K;
+        if (t.ncand == 0) t.cand[t.ncand++] = kmin;
+        t.best = t.cand[0];
+    }
+    if (t.ntried < t.ncand) {
+        *state = 1;
+        return t.cand[t.ntried];
+    }
+    *state = 2;
+    return t.best;
+}
+
+void ktune_record(int device, uint64_t key, int32_t K, float ms, double rec) {
+    std::lock_guard<std::mutex> g(g_ktune_mu);
+    KTune& t = g_ktune[device & 15];
+    if (t.key != key || t.ntried >= t.ncand || t.cand[t.ntried] != K) return;
+    t.ms[t.ntried] = ms;
+    t.rec[t.ntried] = rec;
+    if (++t.ntried == t.ncand) {
+        int bi = -1;
+        for (int k = 0; k < t.ncand; ++k)
+            if (t.rec[k] <= kRecTol && (bi < 0 || t.ms[k] < t.ms[bi])) bi = k;
+        if (bi < 0) bi = 0;
+        t.best = t.cand[bi];
+        t.best_ms = t.ms[bi];
+    }
+}
+
+float ktune_best_ms(int device, uint64_t key) {
+    std::lock_guard<std::mutex> g(g_ktune_mu);
+    const KTune& t = g_ktune[device & 15];
+    return t.key == key ? t.best_ms : 0.f;
+}
+
 // The shared driver.  coords0/lost0 are device pointers here.
 int run_adjoint(tp_ctx* c, const std::vector<const tp_lattice*>& lats, const std::vector<int64_t>& npart,
                 const std::vector<double>& betis, const double* d_coords0, const int64_t* d_lost0, int32_t nturns,
@@ -590,7 +665,17 @@ int run_adjoint(tp_ctx* c, const std::vector<const tp_lattice*>& lats, const std
     int st = make_plan(lats, npart, betis, params, poff_params, turn0, nturns, &P);
     if (st != TP_OK) return st;
     const int nvar = int(lats.size());
-    if (K <= 0) K = auto_interval(P.ntot, nturns);
+    CtxHost ch0;
+    ctx_host(c, &ch0);
+    int kstate = 0;  // 0: K fixed by the caller (or a loss-only call); 1: tuning trial; 2: tuned
+    uint64_t kkey = 0;
+    if (K <= 0 && mode == 0) {
+        kkey = ktune_key({P.ntot, nturns, nvar, int64_t(P.table.size()), int64_t(P.param_off.back()), int64_t(exact),
+                          int64_t(P.sched.size()), int64_t(P.mis.size())});
+        K = ktune_pick(ch0.device, kkey, P.ntot, nturns, &kstate);
+    } else if (K <= 0) {
+        K = auto_interval(P.ntot, nturns);
+    }
     K = std::max(1, std::min(K, std::max(nturns, 1)));
     const int32_t nseg = nturns > 0 ? (nturns + K - 1) / K : 1;
     CtxHost ch;
@@ -756,6 +841,9 @@ int run_adjoint(tp_ctx* c, const std::vector<const tp_lattice*>& lats, const std
     g_adj_stats.particles = P.ntot;
     g_adj_stats.launches = 2 + (mode == 0 ? 1 : 0);
     g_adj_stats.units = u;
+    if (kstate == 1) ktune_record(ch0.device, kkey, K, *ms_fwd + *ms_rev, m);
+    g_adj_stats.k_tuning = kstate;
+    g_adj_stats.tuned_ms = kstate ? ktune_best_ms(ch0.device, kkey) : 0.0;
     return TP_OK;
 }
 
@@ -806,6 +894,7 @@ TP_API int tp_ringpass_adjoint(tp_ctx* ctx, const tp_lattice* lat, const double*
                                int32_t turn0, const int32_t* param_elems, int32_t nparams, const tp_loss_spec* loss,
                                int32_t checkpoint_every, double* loss_out, double* grad_out, double* coords_out,
                                int64_t* lost_out, const tp_opts* opts) {
+    tp::NvtxRange nvtx_range("tp_ringpass_adjoint");
     (void)time;
     (void)dt_turn;
     auto t0 = std::chrono::steady_clock::now();
@@ -867,7 +956,7 @@ TP_API int tp_ringpass_adjoint(tp_ctx* ctx, const tp_lattice* lat, const double*
     S.h2d_bytes = h2d;
     S.d2h_bytes = d2h + 8 * (1 + nparams);
     S.block_size = kAdjBlock;
-    S.ppt = 1;
+    S.min_blocks = 4;
     S.launches = g_adj_stats.launches;
     S.schedule = 1;
     return TP_OK;
@@ -878,6 +967,7 @@ TP_API int tp_ringpass_adjoint_batched(tp_ctx* ctx, tp_batch* b, const double* c
                                        double dt_turn, int32_t turn0, const int32_t* param_elems,
                                        const int32_t* param_off, const tp_loss_spec* loss, int32_t checkpoint_every,
                                        double* loss_out, double* grad_out, const tp_opts* opts) {
+    tp::NvtxRange nvtx_range("tp_ringpass_adjoint_batched");
     (void)time;
     (void)dt_turn;
     auto t0 = std::chrono::steady_clock::now();
@@ -936,7 +1026,7 @@ TP_API int tp_ringpass_adjoint_batched(tp_ctx* ctx, tp_batch* b, const double* c
     S.h2d_bytes = h2d;
     S.d2h_bytes = 8 * (nvar + pofs[size_t(nvar)]);
     S.block_size = kAdjBlock;
-    S.ppt = 1;
+    S.min_blocks = 4;
     S.launches = g_adj_stats.launches;
     S.schedule = 1;
     return TP_OK;
@@ -945,6 +1035,7 @@ TP_API int tp_ringpass_adjoint_batched(tp_ctx* ctx, tp_batch* b, const double* c
 TP_API int tp_one_turn_jacobian(tp_ctx* ctx, const tp_lattice* lat, const double* orbits, int64_t n, double beti,
                                 int32_t nturns, int32_t turn0, double* jac_out, double* sympl_out,
                                 const tp_opts* opts) {
+    tp::NvtxRange nvtx_range("tp_one_turn_jacobian");
     auto t0 = std::chrono::steady_clock::now();
     if (!ctx || !lat) return fail(TP_EINVAL, "null context or lattice");
     if (n < 0 || nturns < 0) return fail(TP_EINVAL, "negative size");
@@ -1012,7 +1103,7 @@ TP_API int tp_one_turn_jacobian(tp_ctx* ctx, const tp_lattice* lat, const double
     S.h2d_bytes = h2d;
     S.d2h_bytes = d2h;
     S.block_size = kAdjBlock;
-    S.ppt = 1;
+    S.min_blocks = 4;
     S.launches = 2 + 2;
     S.schedule = 1;
     return TP_OK;

@@ -75,12 +75,18 @@ enum DevErr : int32_t {
 bool records_have_rare(const double* recs, size_t words);
 
 // Kernel launchers (tp_track.cu, compiled once with and once without FMA
-// contraction).  Return a cudaError_t value.
+// contraction).  Return a cudaError_t value.  `minb` selects the kernel
+// instance whose registers are sized for that many resident 128-thread blocks
+// per SM (5, 6 or 7 in the build without contraction, 7 in the other; tables
+// with kinds outside the integrator core always run 7); minb_track_* maps a
+// request to the instance that runs.
 constexpr int kTrackMaxBlock = 128;  // launch bound of the tracking kernels
-int launch_track_fast(const TrackArgs& a, int grid, int block, int ppt, size_t smem, void* stream);
-int launch_track_strict(const TrackArgs& a, int grid, int block, int ppt, size_t smem, void* stream);
-int occupancy_track_fast(int block, int ppt, size_t smem, int* blocks_per_sm);
-int occupancy_track_strict(int block, int ppt, size_t smem, int* blocks_per_sm);
+int launch_track_fast(const TrackArgs& a, int grid, int block, int minb, size_t smem, void* stream);
+int launch_track_strict(const TrackArgs& a, int grid, int block, int minb, size_t smem, void* stream);
+int occupancy_track_fast(int block, int minb, size_t smem, int* blocks_per_sm);
+int occupancy_track_strict(int block, int minb, size_t smem, int* blocks_per_sm);
+int minb_track_fast(int minb);
+int minb_track_strict(int minb);
 
 // Read-only view of a lattice's compiled program (tp_runtime.cu).  The
 // program may be rebuilt by tp_lattice_set_schedule: hold lattice_mutex(lat)
@@ -131,5 +137,14 @@ void batch_lattices(const tp_batch* b, std::vector<const tp_lattice*>* out);
 
 // Set the text returned by tp_last_error_string on this thread.
 void set_last_error(const std::string& msg);
+
+// A named NVTX range over one entry point (shown by Nsight Systems and by
+// ncu's --nvtx filters; a no-op unless a tool is attached).
+struct NvtxRange {
+    explicit NvtxRange(const char* name);
+    ~NvtxRange();
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 }  // namespace tp

@@ -137,11 +137,11 @@ TP_API int tp_ringpass_noalloc(const tp_lattice* lat, double* coords, int64_t n,
     const size_t smem = 0;
     const int block = 128;
     int bps = 0;
-    if (tp::occupancy_track_strict(block, 1, smem, &bps) != 0 || bps <= 0) bps = 1;
+    if (tp::occupancy_track_strict(block, 0, smem, &bps) != 0 || bps <= 0) bps = 1;
     const int64_t needed = (n + block - 1) / block;
     int grid = a.refill ? int(std::min<int64_t>(int64_t(sm) * bps, needed)) : int(needed);
     if (grid < 1) grid = 1;
-    int le = tp::launch_track_strict(a, grid, block, 1, smem, s);
+    int le = tp::launch_track_strict(a, grid, block, 0, smem, s);
     if (le != 0) return cuda_fail(cudaError_t(le), "track kernel launch");
     int32_t err = 0;
     e = cudaMemcpyAsync(&err, a.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s);

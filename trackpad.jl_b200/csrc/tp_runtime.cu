@@ -18,6 +18,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "tp_internal.h"
 
 using namespace tp;
@@ -44,16 +46,25 @@ int cuda_err(cudaError_t e, const char* where) {
 
 constexpr int kMaxDevices = 16;
 
-// Online choice of the particle scheduling (1 = static, 2 = lane refill).
-// Every schedule gives bit-identical results, so the first two calls of a
-// configuration (same sizes, turns, drift and build) run one schedule each on
-// the caller's own work, timed with the call's CUDA events, and later calls
-// keep the faster one.
-struct SchedTune {
+// Online choice of the launch configuration: the particle scheduling (1 =
+// static, 2 = lane refill) and the kernel instance whose registers are sized
+// for 7, 6 or 5 resident blocks per SM.  Every configuration gives
+// bit-identical results, so the first calls of a configuration key (sizes,
+// turns, drift, build, lattice version) each run one candidate on the caller's
+// own work, timed with the call's CUDA events: first the two schedules at 7
+// resident blocks, then 6 and 5 with the faster schedule.  Later calls keep the
+// fastest candidate.  What the caller fixes in tp_opts is not tuned.
+struct LaunchCand {
+    int sched = 1, minb = 7;
+};
+
+struct LaunchTune {
     uint64_t key = 0;
-    int trials = 0;
-    float ms[2] = {0.f, 0.f};
-    int best = 1;
+    LaunchCand cand[6];
+    float ms[6] = {};
+    int ncand = 0, ntried = 0;
+    bool staged = false;  // the resident-block candidates have been appended
+    LaunchCand best;
 };
 
 uint64_t tune_key(std::initializer_list<int64_t> parts) {
@@ -67,18 +78,74 @@ uint64_t tune_key(std::initializer_list<int64_t> parts) {
     return h | 1ull;
 }
 
-int tune_pick(SchedTune& t, uint64_t key) {
+// The candidate for this call.  fixed_sched / fixed_minb: the caller's choice
+// (0: tuned).  minbs[0..nminb): the resident-block counts the kernel build
+// carries, the default first.  *trial is set when the call is a timing trial.
+LaunchCand tune_pick(LaunchTune& t, uint64_t key, int fixed_sched, int fixed_minb, const int* minbs, int nminb,
+                     bool* trial) {
     if (t.key != key) {
-        t = SchedTune{};
+        t = LaunchTune{};
         t.key = key;
+        const int m0 = fixed_minb ? fixed_minb : minbs[0];
+        if (fixed_sched) {
+            t.cand[t.ncand++] = {fixed_sched, m0};
+        } else {
+            t.cand[t.ncand++] = {1, m0};
+            t.cand[t.ncand++] = {2, m0};
+        }
+        t.staged = fixed_minb != 0 || nminb <= 1;
     }
-    return t.trials < 2 ? 1 + t.trials : t.best;
+    if (t.ntried == t.ncand && !t.staged) {
+        int bi = 0;
+        for (int k = 1; k < t.ntried; ++k)
+            if (t.ms[k] < t.ms[bi]) bi = k;
+        for (int k = 1; k < nminb && t.ncand < 6; ++k) t.cand[t.ncand++] = {t.cand[bi].sched, minbs[k]};
+        t.staged = true;
+    }
+    if (t.ntried < t.ncand) {
+        *trial = true;
+        return t.cand[t.ntried];
+    }
+    *trial = false;
+    return t.best;
 }
 
-void tune_record(SchedTune& t, uint64_t key, int schedule, float ms) {
-    if (t.key != key || t.trials >= 2 || schedule != 1 + t.trials) return;
-    t.ms[schedule - 1] = ms;
-    if (++t.trials == 2) t.best = t.ms[1] < t.ms[0] ? 2 : 1;
+void tune_record(LaunchTune& t, uint64_t key, LaunchCand c, float ms) {
+    if (t.key != key || t.ntried >= t.ncand) return;
+    if (t.cand[t.ntried].sched != c.sched || t.cand[t.ntried].minb != c.minb) return;
+    t.ms[t.ntried++] = ms;
+    if (t.ntried == t.ncand && t.staged) {
+        int bi = 0;
+        for (int k = 1; k < t.ntried; ++k)
+            if (t.ms[k] < t.ms[bi]) bi = k;
+        t.best = t.cand[bi];
+    }
+}
+
+// The launch configuration of one tracking call: the caller's choices, else
+// the tuner's (multi-turn tracks only; single passes run static at the
+// default).  Returns whether the call is a timing trial.
+bool pick_launch(LaunchTune* tu, std::mutex* mu, uint64_t key, const tp_opts& o, int nturns, bool strict, bool rare,
+                 LaunchCand* out) {
+    int minbs[3] = {7, 6, 5};
+    int nminb = 1;
+    if (strict && !rare && minb_track_strict(5) == 5 && minb_track_strict(6) == 6) nminb = 3;
+    const int fixed_minb = o.min_blocks > 0 ? (strict ? minb_track_strict(o.min_blocks)
+                                                      : minb_track_fast(o.min_blocks)) : 0;
+    const int fixed_sched = o.schedule == 1 || o.schedule == 2 ? o.schedule : 0;
+    if (nturns <= 1 || (fixed_sched && (fixed_minb || nminb == 1))) {
+        out->sched = fixed_sched ? fixed_sched : 1;
+        out->minb = fixed_minb ? fixed_minb : minbs[0];
+        return false;
+    }
+    bool trial = false;
+    if (mu) {
+        std::lock_guard<std::mutex> g(*mu);
+        *out = tune_pick(*tu, key, fixed_sched, fixed_minb, minbs, nminb, &trial);
+    } else {
+        *out = tune_pick(*tu, key, fixed_sched, fixed_minb, minbs, nminb, &trial);
+    }
+    return trial;
 }
 
 std::atomic<uint64_t> g_stamp{0};
@@ -92,7 +159,7 @@ struct DevLattice {
     double* prefix = nullptr;  // inclusive prefix sums of per-element flops
     size_t sched_bytes = 0;
     uint64_t version = 0;
-    SchedTune tune;
+    LaunchTune tune;
 };
 
 }  // namespace
@@ -140,7 +207,7 @@ struct tp_batch {
     int64_t* sched_v = nullptr;        // per variant: word offset (-1: none), stride, first turn, turns
     std::vector<uint64_t> h_ver;       // lattice versions the device tables were built from
     unsigned long long* pool = nullptr; // per variant particles handed out (pooled refill)
-    SchedTune tune;
+    LaunchTune tune;
     std::vector<int64_t> h_sched_v;
     // cached CUDA graph of the launch sequence and every value it bakes in
     // (argument values, device pointers, launch shapes; see graph_key)
@@ -411,6 +478,9 @@ int ctx_scratch(tp_ctx* c, int slot, size_t bytes, void** out) {
 void batch_lattices(const tp_batch* b, std::vector<const tp_lattice*>* out) { *out = b->lats; }
 
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+
+NvtxRange::NvtxRange(const char* name) { nvtxRangePushA(name); }
+NvtxRange::~NvtxRange() { nvtxRangePop(); }
 
 }  // namespace tp
 
@@ -734,29 +804,22 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     const size_t table_bytes = L->program.size() * sizeof(double);
     const size_t smem = o.table_in_smem && table_bytes + 64 <= c->smem_optin ? table_bytes : 0;
     a.smem_words = smem ? int32_t(L->program.size()) : 0;
-    // Launch configuration: static for single passes; for multi-turn tracks the
-    // schedule the caller asks for, else the tuned one (lane refill frees the
-    // lanes of lost particles, static has less bookkeeping).
+    // Launch configuration: static at the default occupancy for single passes;
+    // for multi-turn tracks what the caller asks for, else the tuned choice
+    // (lane refill frees the lanes of lost particles, static has less
+    // bookkeeping; more resident blocks hide more latency, fewer spill less).
     int block = o.block_size > 0 ? o.block_size : 128;
     block = std::max(32, std::min(kTrackMaxBlock, block / 32 * 32));
     const bool strict = o.fp_contract == 0;
     const uint64_t tkey = tune_key({n, nturns, int64_t(exact), int64_t(strict), block, int64_t(L->version),
-                                    int64_t(L->program.size())});
-    bool tuning = false;
-    int schedule = o.schedule;
-    if (schedule == 0) {
-        if (nturns <= 1) {
-            schedule = 1;
-        } else {
-            std::lock_guard<std::mutex> g(L->mu);
-            SchedTune& tu = L->dev[c->device].tune;
-            schedule = tune_pick(tu, tkey);
-            tuning = tu.trials < 2;
-        }
-    }
+                                    int64_t(L->program.size()), int64_t(smem)});
+    LaunchCand lc;
+    const bool tuning = pick_launch(&L->dev[c->device].tune, &L->mu, tkey, o, nturns, strict, a.rare != 0, &lc);
+    const int schedule = lc.sched;
     a.refill = schedule == 2 ? 1 : 0;
     int bps = 0;
-    int oerr = strict ? occupancy_track_strict(block, 1, smem, &bps) : occupancy_track_fast(block, 1, smem, &bps);
+    int oerr = strict ? occupancy_track_strict(block, lc.minb, smem, &bps)
+                      : occupancy_track_fast(block, lc.minb, smem, &bps);
     if (oerr != 0 || bps <= 0) bps = 1;
     int64_t grid_needed = (n + block - 1) / block;
     int grid = a.refill ? int(std::min<int64_t>(int64_t(c->sm_count) * bps, grid_needed)) : int(grid_needed);
@@ -771,7 +834,8 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     k_alive_mask<<<sg, 256, 0, s>>>(d_lost, n, c->alive0, c->counters + 2);
     TP_CUDA(cudaGetLastError());
     TP_CUDA(cudaEventRecord(c->ev0, s));
-    int le = strict ? launch_track_strict(a, grid, block, 1, smem, s) : launch_track_fast(a, grid, block, 1, smem, s);
+    int le = strict ? launch_track_strict(a, grid, block, lc.minb, smem, s)
+                    : launch_track_fast(a, grid, block, lc.minb, smem, s);
     if (le != 0) return cuda_err(cudaError_t(le), "track kernel launch");
     TP_CUDA(cudaEventRecord(c->ev1, s));
     k_work_stats<<<sg, 256, 0, s>>>(c->alive0, d_lost, d_lt, d_le, n, prefix, nullptr, nullptr, nullptr, 0, a.nelem,
@@ -795,7 +859,7 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     TP_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     if (tuning) {
         std::lock_guard<std::mutex> g(L->mu);
-        tune_record(L->dev[c->device].tune, tkey, schedule, ms);
+        tune_record(L->dev[c->device].tune, tkey, lc, ms);
     }
     tp_stats& S = c->stats;
     S.particles = int64_t(cnt[2]);
@@ -808,7 +872,7 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     S.h2d_bytes = h2d;
     S.d2h_bytes = d2h;
     S.block_size = block;
-    S.ppt = 1;
+    S.min_blocks = strict ? minb_track_strict(lc.minb) : minb_track_fast(lc.minb);
     S.grid = grid;
     S.launches = 3 + (lost_turn ? 0 : 1) + (lost_elem ? 0 : 1);
     S.schedule = schedule;
@@ -819,6 +883,7 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
 TP_API int tp_linepass(tp_ctx* c, const tp_lattice* L, double* coords, int64_t n, int64_t* lost_flags,
                        int32_t* lost_turn, int32_t* lost_elem, double beti, double time, int32_t turn,
                        const tp_opts* opts) {
+    NvtxRange r("tp_linepass");
     (void)time;  // the host evaluates time-dependent fields into the per-turn schedule
     return track_common(c, const_cast<tp_lattice*>(L), coords, n, lost_flags, lost_turn, lost_elem, beti, 1, turn,
                         opts);
@@ -827,6 +892,7 @@ TP_API int tp_linepass(tp_ctx* c, const tp_lattice* L, double* coords, int64_t n
 TP_API int tp_ringpass(tp_ctx* c, const tp_lattice* L, double* coords, int64_t n, int64_t* lost_flags,
                        int32_t* lost_turn, int32_t* lost_elem, double beti, int32_t nturns, double time,
                        double dt_turn, int32_t turn0, const tp_opts* opts) {
+    NvtxRange r("tp_ringpass");
     (void)time;
     (void)dt_turn;
     return track_common(c, const_cast<tp_lattice*>(L), coords, n, lost_flags, lost_turn, lost_elem, beti, nturns,
@@ -986,6 +1052,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
                                int32_t* lost_turn, int32_t* lost_elem, const double* beti, int32_t nturns,
                                double time, double dt_turn, int32_t turn0, int32_t use_graph,
                                const tp_opts* opts_in) {
+    NvtxRange r("tp_ringpass_batched");
     (void)time;
     (void)dt_turn;
     auto t_start = std::chrono::steady_clock::now();
@@ -1093,19 +1160,12 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     int64_t ph = 0;
     for (int32_t v = 0; v <= nvar; ++v) ph = ph * 1000003 + poff[v];
     const uint64_t tkey = tune_key({n, nturns, int64_t(exact), int64_t(strict), block, ph, int64_t(b->table_words)});
-    bool tuning = false;
-    int schedule = o.schedule;
-    if (schedule == 0) {
-        if (nturns <= 1) {
-            schedule = 1;
-        } else {
-            schedule = tune_pick(b->tune, tkey);
-            tuning = b->tune.trials < 2;
-        }
-    }
+    LaunchCand lc;
+    const bool tuning = pick_launch(&b->tune, nullptr, tkey, o, nturns, strict, a.rare != 0, &lc);
+    const int schedule = lc.sched;
     a.refill = schedule == 2 ? 1 : 0;
     int bps = 0;
-    int oerr = strict ? occupancy_track_strict(block, 1, 0, &bps) : occupancy_track_fast(block, 1, 0, &bps);
+    int oerr = strict ? occupancy_track_strict(block, lc.minb, 0, &bps) : occupancy_track_fast(block, lc.minb, 0, &bps);
     if (oerr != 0 || bps <= 0) bps = 1;
     int grid = int(std::min<int64_t>(int64_t(c->sm_count) * bps, (tiles * 32 + block - 1) / block));
     grid = std::max(grid, 1);
@@ -1124,7 +1184,8 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
         k_alive_mask<<<sg, 256, 0, q>>>(d_lost, n, c->alive0, c->counters + 2);
         TP_CUDA(cudaGetLastError());
         if (timed) TP_CUDA(cudaEventRecord(c->ev0, q));
-        int le = strict ? launch_track_strict(a, grid, block, 1, 0, q) : launch_track_fast(a, grid, block, 1, 0, q);
+        int le = strict ? launch_track_strict(a, grid, block, lc.minb, 0, q)
+                        : launch_track_fast(a, grid, block, lc.minb, 0, q);
         if (le != 0) return cuda_err(cudaError_t(le), "batched track kernel launch");
         if (timed) TP_CUDA(cudaEventRecord(c->ev1, q));
         k_work_stats<<<sg, 256, 0, q>>>(c->alive0, d_lost, d_lt, d_le, n, d_pre, b->poff, d_pre_off, b->nelem_v, nvar,
@@ -1147,7 +1208,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
             u(b->sched_v), u(b->pool), u(b->prefix), u(b->prefix_off), u(d_pre),
             uint64_t(uint32_t(nturns)), uint64_t(uint32_t(turn0)), uint64_t(exact), uint64_t(strict),
             uint64_t(a.refill), uint64_t(a.rare), dbits(a.limx), dbits(a.limy), dbits(a.beti),
-            uint64_t(block), uint64_t(grid), uint64_t(sg), uint64_t(n)};
+            uint64_t(block), uint64_t(grid), uint64_t(sg), uint64_t(n), uint64_t(lc.minb)};
         for (int32_t v = 0; v <= nvar; ++v) key.push_back(uint64_t(poff[v]));
         if (!b->graph || b->g_key != key) {
             if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
@@ -1190,7 +1251,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     if (st != TP_OK) return st;
     float ms = 0.f;
     TP_CUDA(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
-    if (tuning) tune_record(b->tune, tkey, schedule, ms);
+    if (tuning) tune_record(b->tune, tkey, lc, ms);
     tp_stats& S = c->stats;
     S.particles = int64_t(cnt[2]);
     S.survivors = int64_t(cnt[3]);
@@ -1202,7 +1263,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     S.h2d_bytes = h2d;
     S.d2h_bytes = d2h;
     S.block_size = block;
-    S.ppt = 1;
+    S.min_blocks = strict ? minb_track_strict(lc.minb) : minb_track_fast(lc.minb);
     S.grid = grid;
     S.launches = 3 + ((dev && lost_turn) ? 0 : 1) + ((dev && lost_elem) ? 0 : 1);
     S.schedule = schedule;

@@ -1031,6 +1031,7 @@ TP_API int tp_tpsa_monomials(int32_t order, int32_t* exps) {
 
 TP_API int tp_tpsa_ringpass(tp_ctx* ctx, const tp_lattice* lat, double* maps, int64_t nmaps, int32_t order,
                             double beti, int32_t nturns, int32_t turn0) {
+    tp::NvtxRange nvtx_range("tp_tpsa_ringpass");
     if (!ctx || !lat) return fail(TP_EINVAL, "null context or lattice");
     if (order < 0 || order > kTpsaMaxOrder) return fail(TP_ERANGE, "TPSA order outside 0..10");
     if (nmaps < 0 || nturns < 0) return fail(TP_EINVAL, "negative size");

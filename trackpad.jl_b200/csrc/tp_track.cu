@@ -40,13 +40,16 @@ using namespace tp::dev;
 #ifndef TP_MAX_BLOCK
 #define TP_MAX_BLOCK 128
 #endif
-// Resident 128-thread blocks per SM the register allocation is sized for: 7
-// gives 72 registers and 28 warps per SM.  Measured on the DBA step with the
-// element table read through L1 (where the spilled stack lives): 4 blocks
-// 697 ms, 5 blocks 638 ms, 6 blocks 626 ms, 7 blocks 611 ms, 8 blocks 630 ms.
-#ifndef TP_MIN_BLOCKS
-#define TP_MIN_BLOCKS 7
-#endif
+// Resident 128-thread blocks per SM the register allocation is sized for
+// (MINB, a template parameter of the kernels): 7 gives 72 registers and 28
+// warps per SM, 6 gives 80 registers, 5 gives 96.  Measured on the DBA step
+// with the element table read through L1 (where the spilled stack lives): 4
+// blocks 697 ms, 5 blocks 638 ms, 6 blocks 626 ms, 7 blocks 611 ms, 8 blocks
+// 630 ms.  Fewer registers spill more, more warps hide more latency; which
+// wins depends on the lattice and the schedule, so the build that runs the
+// reference's operation order (TP_OCC_VARIANTS) carries 5, 6 and 7 for the
+// integrator-core kernels and the host picks one by timing.
+constexpr int kMinBlocksDefault = 7;
 constexpr int kMaxBlock = TP_MAX_BLOCK;
 constexpr long long kTmaSpinLimit = 1ll << 22;  // bounded mbarrier wait
 
@@ -216,8 +219,8 @@ __device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, doubl
     }
 }
 
-template <bool EXACT, bool REFILL, bool RARE>
-__global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_single(TrackArgs a) {
+template <bool EXACT, bool REFILL, bool RARE, int MINB>
+__global__ void __launch_bounds__(kMaxBlock, MINB) track_single(TrackArgs a) {
     extern __shared__ __align__(16) double smem[];
     __shared__ __align__(8) uint64_t mbar;
     const double* tab = a.table;
@@ -260,8 +263,8 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_single(TrackAr
 // refills lanes freed by a loss at turn boundaries until the pool is empty;
 // later tiles of an emptied variant end at once.  Either way every particle is
 // tracked from turn 0 with its own turn counter, so the results are the same.
-template <bool EXACT, bool REFILL, bool RARE>
-__global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_batched(TrackArgs a, const int64_t* tile_off) {
+template <bool EXACT, bool REFILL, bool RARE, int MINB>
+__global__ void __launch_bounds__(kMaxBlock, MINB) track_batched(TrackArgs a, const int64_t* tile_off) {
     const int lane = threadIdx.x & 31;
     const int64_t ntiles = tile_off[a.nvar];
     for (;;) {
@@ -307,57 +310,88 @@ __global__ void __launch_bounds__(kMaxBlock, TP_MIN_BLOCKS) track_batched(TrackA
     }
 }
 
-// The kernel instance of (exact drift, refill, rare kinds) chosen at run time.
-template <bool EXACT, bool REFILL, bool RARE>
+// The kernel instance of (exact drift, refill, rare kinds, resident blocks)
+// chosen at run time.
+template <bool EXACT, bool REFILL, bool RARE, int MINB>
 int launch_t(const TrackArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
     if (a.nvar > 0) {
         const int64_t* tile_off = a.toff + (a.nvar + 1);  // host packs tile offsets and the order after toff
-        track_batched<EXACT, REFILL, RARE><<<grid, block, 0, st>>>(a, tile_off);
+        track_batched<EXACT, REFILL, RARE, MINB><<<grid, block, 0, st>>>(a, tile_off);
         return int(cudaGetLastError());
     }
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(track_single<EXACT, REFILL, RARE>,
+        cudaError_t e = cudaFuncSetAttribute(track_single<EXACT, REFILL, RARE, MINB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return int(e);
     }
-    track_single<EXACT, REFILL, RARE><<<grid, block, smem, st>>>(a);
+    track_single<EXACT, REFILL, RARE, MINB><<<grid, block, smem, st>>>(a);
     return int(cudaGetLastError());
 }
 
+// Resident-block counts this build carries for the integrator-core kernels
+// (tables with rare kinds always use the default).
+int clamp_minb(int minb) {
+#ifdef TP_OCC_VARIANTS
+    return (minb == 5 || minb == 6) ? minb : kMinBlocksDefault;
+#else
+    (void)minb;
+    return kMinBlocksDefault;
+#endif
+}
+
 template <bool EXACT, bool REFILL>
-int launch_r(const TrackArgs& a, int grid, int block, size_t smem, cudaStream_t st) {
-    return a.rare ? launch_t<EXACT, REFILL, true>(a, grid, block, smem, st)
-                  : launch_t<EXACT, REFILL, false>(a, grid, block, smem, st);
+int launch_r(const TrackArgs& a, int grid, int block, int minb, size_t smem, cudaStream_t st) {
+    if (a.rare) return launch_t<EXACT, REFILL, true, kMinBlocksDefault>(a, grid, block, smem, st);
+#ifdef TP_OCC_VARIANTS
+    if (minb == 5) return launch_t<EXACT, REFILL, false, 5>(a, grid, block, smem, st);
+    if (minb == 6) return launch_t<EXACT, REFILL, false, 6>(a, grid, block, smem, st);
+#endif
+    (void)minb;
+    return launch_t<EXACT, REFILL, false, kMinBlocksDefault>(a, grid, block, smem, st);
 }
 
-int launch(const TrackArgs& a, int grid, int block, int ppt, size_t smem, void* stream) {
-    (void)ppt;
+int launch(const TrackArgs& a, int grid, int block, int minb, size_t smem, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    minb = a.rare ? kMinBlocksDefault : clamp_minb(minb);
     if (a.nvar > 0) smem = 0;
-    if (a.exact && a.refill) return launch_r<true, true>(a, grid, block, smem, st);
-    if (a.exact) return launch_r<true, false>(a, grid, block, smem, st);
-    if (a.refill) return launch_r<false, true>(a, grid, block, smem, st);
-    return launch_r<false, false>(a, grid, block, smem, st);
+    if (a.exact && a.refill) return launch_r<true, true>(a, grid, block, minb, smem, st);
+    if (a.exact) return launch_r<true, false>(a, grid, block, minb, smem, st);
+    if (a.refill) return launch_r<false, true>(a, grid, block, minb, smem, st);
+    return launch_r<false, false>(a, grid, block, minb, smem, st);
 }
 
-int occupancy(int block, int ppt, size_t smem, int* blocks_per_sm) {
-    (void)ppt;
+template <int MINB>
+int occupancy_t(int block, size_t smem, int* blocks_per_sm) {
     if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(track_single<true, true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+        cudaError_t e = cudaFuncSetAttribute(track_single<true, true, false, MINB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
         if (e != cudaSuccess) return int(e);
     }
-    return int(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, track_single<true, true, false>, block, smem));
+    return int(cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, track_single<true, true, false, MINB>,
+                                                             block, smem));
 }
+
+int occupancy(int block, int minb, size_t smem, int* blocks_per_sm) {
+    minb = clamp_minb(minb);
+#ifdef TP_OCC_VARIANTS
+    if (minb == 5) return occupancy_t<5>(block, smem, blocks_per_sm);
+    if (minb == 6) return occupancy_t<6>(block, smem, blocks_per_sm);
+#endif
+    return occupancy_t<kMinBlocksDefault>(block, smem, blocks_per_sm);
+}
+
+int carried_minb(int minb) { return clamp_minb(minb); }
 
 }  // namespace TP_NS
 
 #define TP_CAT2(a, b) a##_##b
 #define TP_CAT(a, b) TP_CAT2(a, b)
-int TP_CAT(launch_track, TP_NS)(const TrackArgs& a, int grid, int block, int ppt, size_t smem, void* stream) {
-    return TP_NS::launch(a, grid, block, ppt, smem, stream);
+int TP_CAT(launch_track, TP_NS)(const TrackArgs& a, int grid, int block, int minb, size_t smem, void* stream) {
+    return TP_NS::launch(a, grid, block, minb, smem, stream);
 }
-int TP_CAT(occupancy_track, TP_NS)(int block, int ppt, size_t smem, int* blocks_per_sm) {
-    return TP_NS::occupancy(block, ppt, smem, blocks_per_sm);
+int TP_CAT(occupancy_track, TP_NS)(int block, int minb, size_t smem, int* blocks_per_sm) {
+    return TP_NS::occupancy(block, minb, smem, blocks_per_sm);
 }
+int TP_CAT(minb_track, TP_NS)(int minb) { return TP_NS::carried_minb(minb); }
 
 }  // namespace tp

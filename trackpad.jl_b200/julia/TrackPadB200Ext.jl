@@ -37,7 +37,7 @@ end
 
 struct TpOpts
     size::Int32; exact_hamiltonian::Int32; device_pointers::Int32; fp_contract::Int32
-    block_size::Int32; ppt::Int32; schedule::Int32; table_in_smem::Int32
+    block_size::Int32; min_blocks::Int32; schedule::Int32; table_in_smem::Int32
     aperture_x::Float64; aperture_y::Float64; stream::Ptr{Cvoid}
 end
 
