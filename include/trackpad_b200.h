@@ -207,6 +207,12 @@ typedef struct tp_opts {
     void* stream;              /* cudaStream_t to run on; NULL = context stream, a
                                   blocking stream ordered with the legacy default
                                   stream                                          */
+    int32_t bounds_check;      /* 1: run the bounds-checked tracking kernels (no
+                                  FMA contraction): an element-table record outside
+                                  its table or turn block, or a particle index >= N,
+                                  is skipped and reported as TP_EDEVICE instead of
+                                  being read; results are otherwise identical      */
+    int32_t reserved0;
 } tp_opts;
 
 /* Statistics of the last tracking call on a context. */

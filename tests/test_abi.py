@@ -32,10 +32,32 @@ def test_library_exports_every_header_symbol():
         assert hasattr(lib, n), n
 
 
-def test_struct_layouts_match_header():
-    assert C.sizeof(abi.TpElem) == 8 * 4 + 33 * 8
-    assert C.sizeof(abi.TpMisalign) == 84 * 8
-    assert C.sizeof(abi.TpOpts) == 8 * 4 + 2 * 8 + 8
+def test_struct_layouts_match_header(tmp_path):
+    """The ctypes declarations have the sizes and field offsets the C compiler
+    gives the header's structs."""
+    import subprocess
+    structs = {"tp_elem": abi.TpElem, "tp_misalign": abi.TpMisalign, "tp_opts": abi.TpOpts, "tp_stats": abi.TpStats,
+               "tp_loss_spec": abi.TpLossSpec, "tp_adjoint_stats": abi.TpAdjointStats,
+               "tp_tpsa_stats": abi.TpTpsaStats}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "trackpad_b200.h"', "int main(void) {"]
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} @sizeof %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    seen = 0
+    for line in filter(None, out):
+        cname, what, val = line.split()
+        py = structs[cname]
+        got = C.sizeof(py) if what == "@sizeof" else getattr(py, what).offset
+        assert got == int(val), (cname, what, got, val)
+        seen += 1
+    assert seen == sum(1 + len(p._fields_) for p in structs.values())
 
 
 def test_version_and_strerror():

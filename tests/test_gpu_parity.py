@@ -454,3 +454,36 @@ def test_table_in_shared_memory_or_l1_gives_the_same_bits():
     (c1, l1, s1, g1), (c2, l2, s2, g2) = out
     assert np.array_equal(c1, c2, equal_nan=True) and np.array_equal(l1, l2)
     assert s1 == s2 and np.array_equal(g1, g2)
+
+
+def test_bounds_checked_kernels_give_the_same_bits():
+    """tp_opts.bounds_check runs the kernels that check every element-table
+    record (inside its table or turn block) and particle index before reading
+    them: on valid inputs they give the default build's bits, single lattice
+    (with a per-turn schedule) and batched, and report no violation."""
+    base = W.dba_ring(cells=2)
+    lat = W.time_dependent(base, 8)
+    beam = W.dba_beam()
+    c0 = np.asfortranarray(np.concatenate([W.gaussian(400, seed=90), W.da_grid(10, 10)]))
+    outs = []
+    for bc in (False, True):
+        c = c0.copy(order="F")
+        l = np.zeros(len(c), np.int64)
+        lt = np.full(len(c), -1, np.int32)
+        tp.ringpass_(c, lat, beam, l, 8, aperture=0.02, lost_turn=lt, bounds_check=bc)
+        outs.append((c, l, lt))
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+    variants = W.dba_variants(nvar=4, seed=14, n_base=150, cells_range=(2, 4))
+    counts = [n for _, n in variants]
+    poff = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    coords = np.asfortranarray(np.concatenate([W.gaussian(n, seed=95 + i) for i, n in enumerate(counts)]))
+    batch = tp.Batch([v for v, _ in variants])
+    bo = []
+    for bc in (False, True):
+        cb = coords.copy(order="F")
+        lb = np.zeros(len(cb), np.int64)
+        batch.ringpass_(cb, poff, np.full(4, tp.beti(beam)), lb, 6, aperture=0.02, schedule=2, use_graph=True,
+                        bounds_check=bc)
+        bo.append((cb, lb))
+    assert np.array_equal(bo[0][0], bo[1][0]) and np.array_equal(bo[0][1], bo[1][1])

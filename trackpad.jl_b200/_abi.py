@@ -64,6 +64,7 @@ class TpOpts(C.Structure):
         ("size", C.c_int32), ("exact_hamiltonian", C.c_int32), ("device_pointers", C.c_int32),
         ("fp_contract", C.c_int32), ("block_size", C.c_int32), ("min_blocks", C.c_int32), ("schedule", C.c_int32),
         ("table_in_smem", C.c_int32), ("aperture_x", C.c_double), ("aperture_y", C.c_double), ("stream", C.c_void_p),
+        ("bounds_check", C.c_int32), ("reserved0", C.c_int32),
     ]
 
 

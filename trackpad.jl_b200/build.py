@@ -1,8 +1,9 @@
 """Build libtrackpad_b200.so in-tree with nvcc for sm_100a.
 
-The tracking kernel is compiled twice: once with FMA contraction (the fast
-build) and once with -fmad=false (the strict build, whose arithmetic matches the
-reference operation for operation).  Host code is compiled without FMA
+The tracking kernel is compiled three times: with FMA contraction (the fast
+build), with -fmad=false (the strict build, whose arithmetic matches the
+reference operation for operation) and strict with bounds checks (the checked
+build, selected per call by tp_opts.bounds_check).  Host code is compiled without FMA
 contraction so that hoisted element constants are bit-identical to the values
 the reference computes per particle.
 """
@@ -43,6 +44,7 @@ def build(verbose=False, ptxas_info=False):
     units = [
         ("tp_track_fast.o", "tp_track.cu", ["-DTP_NS=fast", "-fmad=true"]),
         ("tp_track_strict.o", "tp_track.cu", ["-DTP_NS=strict", "-fmad=false", "-DTP_OCC_VARIANTS"]),
+        ("tp_track_checked.o", "tp_track.cu", ["-DTP_NS=checked", "-fmad=false", "-DTP_BOUNDS_CHECK"]),
         ("tp_runtime.o", "tp_runtime.cu", ["-fmad=false"]),
         ("tp_adjoint.o", "tp_adjoint.cu", ["-fmad=false"]),
         ("tp_compile.o", "tp_compile.cpp", ["-fmad=false", "-x", "cu"]),

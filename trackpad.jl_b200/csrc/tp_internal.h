@@ -67,6 +67,7 @@ enum DevErr : int32_t {
     DE_BAD_KIND = 1,
     DE_SCHED_RANGE = 2,
     DE_TMA_TIMEOUT = 4,
+    DE_BOUNDS = 8,        // bounds-checked build: a table record or particle index out of range
 };
 
 // True when a record of `words` words of records (a compiled table) has a
@@ -87,6 +88,10 @@ int occupancy_track_fast(int block, int minb, size_t smem, int* blocks_per_sm);
 int occupancy_track_strict(int block, int minb, size_t smem, int* blocks_per_sm);
 int minb_track_fast(int minb);
 int minb_track_strict(int minb);
+// The bounds-checked build (no contraction, tp_opts.bounds_check).
+int launch_track_checked(const TrackArgs& a, int grid, int block, int minb, size_t smem, void* stream);
+int occupancy_track_checked(int block, int minb, size_t smem, int* blocks_per_sm);
+int minb_track_checked(int minb);
 
 // Read-only view of a lattice's compiled program (tp_runtime.cu).  The
 // program may be rebuilt by tp_lattice_set_schedule: hold lattice_mutex(lat)

@@ -125,13 +125,39 @@ void tune_record(LaunchTune& t, uint64_t key, LaunchCand c, float ms) {
 // The launch configuration of one tracking call: the caller's choices, else
 // the tuner's (multi-turn tracks only; single passes run static at the
 // default).  Returns whether the call is a timing trial.
-bool pick_launch(LaunchTune* tu, std::mutex* mu, uint64_t key, const tp_opts& o, int nturns, bool strict, bool rare,
-                 LaunchCand* out) {
+// The three builds of the tracking kernels (tp_track.cu): with FMA
+// contraction, without, and without with bounds checks.
+enum TrackBuild { TB_FAST = 0, TB_STRICT = 1, TB_CHECKED = 2 };
+
+TrackBuild track_build(const tp_opts& o) {
+    if (o.bounds_check) return TB_CHECKED;
+    return o.fp_contract ? TB_FAST : TB_STRICT;
+}
+
+int track_launch(TrackBuild b, const TrackArgs& a, int grid, int block, int minb, size_t smem, void* stream) {
+    if (b == TB_CHECKED) return launch_track_checked(a, grid, block, minb, smem, stream);
+    if (b == TB_STRICT) return launch_track_strict(a, grid, block, minb, smem, stream);
+    return launch_track_fast(a, grid, block, minb, smem, stream);
+}
+
+int track_occupancy(TrackBuild b, int block, int minb, size_t smem, int* bps) {
+    if (b == TB_CHECKED) return occupancy_track_checked(block, minb, smem, bps);
+    if (b == TB_STRICT) return occupancy_track_strict(block, minb, smem, bps);
+    return occupancy_track_fast(block, minb, smem, bps);
+}
+
+int track_minb(TrackBuild b, int minb) {
+    if (b == TB_CHECKED) return minb_track_checked(minb);
+    if (b == TB_STRICT) return minb_track_strict(minb);
+    return minb_track_fast(minb);
+}
+
+bool pick_launch(LaunchTune* tu, std::mutex* mu, uint64_t key, const tp_opts& o, int nturns, TrackBuild build,
+                 bool rare, LaunchCand* out) {
     int minbs[3] = {7, 6, 5};
     int nminb = 1;
-    if (strict && !rare && minb_track_strict(5) == 5 && minb_track_strict(6) == 6) nminb = 3;
-    const int fixed_minb = o.min_blocks > 0 ? (strict ? minb_track_strict(o.min_blocks)
-                                                      : minb_track_fast(o.min_blocks)) : 0;
+    if (!rare && track_minb(build, 5) == 5 && track_minb(build, 6) == 6) nminb = 3;
+    const int fixed_minb = o.min_blocks > 0 ? track_minb(build, o.min_blocks) : 0;
     const int fixed_sched = o.schedule == 1 || o.schedule == 2 ? o.schedule : 0;
     if (nturns <= 1 || (fixed_sched && (fixed_minb || nminb == 1))) {
         out->sched = fixed_sched ? fixed_sched : 1;
@@ -409,6 +435,8 @@ double loss_limit(double aperture) { return aperture > 0.0 ? std::min(1.0, apert
 int check_device_error(tp_ctx* c) {
     int32_t err = 0;
     TP_CUDA(cudaMemcpy(&err, c->err, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    if (err & DE_BOUNDS) return set_err(TP_EDEVICE, "bounds check: an element-table record or particle index "
+                                                    "lay outside its array (the access was skipped)");
     if (err & DE_BAD_KIND) return set_err(TP_EUNSUPPORTED, "kernel met an unknown element record");
     if (err & DE_SCHED_RANGE) return set_err(TP_ERANGE, "turn outside the lattice schedule");
     if (err & DE_TMA_TIMEOUT) return set_err(TP_ETIMEOUT, "element-table staging wait ran out");
@@ -810,16 +838,16 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     // bookkeeping; more resident blocks hide more latency, fewer spill less).
     int block = o.block_size > 0 ? o.block_size : 128;
     block = std::max(32, std::min(kTrackMaxBlock, block / 32 * 32));
-    const bool strict = o.fp_contract == 0;
-    const uint64_t tkey = tune_key({n, nturns, int64_t(exact), int64_t(strict), block, int64_t(L->version),
+    const TrackBuild build = track_build(o);
+    const bool strict = build != TB_FAST;
+    const uint64_t tkey = tune_key({n, nturns, int64_t(exact), int64_t(build), block, int64_t(L->version),
                                     int64_t(L->program.size()), int64_t(smem)});
     LaunchCand lc;
-    const bool tuning = pick_launch(&L->dev[c->device].tune, &L->mu, tkey, o, nturns, strict, a.rare != 0, &lc);
+    const bool tuning = pick_launch(&L->dev[c->device].tune, &L->mu, tkey, o, nturns, build, a.rare != 0, &lc);
     const int schedule = lc.sched;
     a.refill = schedule == 2 ? 1 : 0;
     int bps = 0;
-    int oerr = strict ? occupancy_track_strict(block, lc.minb, smem, &bps)
-                      : occupancy_track_fast(block, lc.minb, smem, &bps);
+    int oerr = track_occupancy(build, block, lc.minb, smem, &bps);
     if (oerr != 0 || bps <= 0) bps = 1;
     int64_t grid_needed = (n + block - 1) / block;
     int grid = a.refill ? int(std::min<int64_t>(int64_t(c->sm_count) * bps, grid_needed)) : int(grid_needed);
@@ -834,8 +862,7 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     k_alive_mask<<<sg, 256, 0, s>>>(d_lost, n, c->alive0, c->counters + 2);
     TP_CUDA(cudaGetLastError());
     TP_CUDA(cudaEventRecord(c->ev0, s));
-    int le = strict ? launch_track_strict(a, grid, block, lc.minb, smem, s)
-                    : launch_track_fast(a, grid, block, lc.minb, smem, s);
+    int le = track_launch(build, a, grid, block, lc.minb, smem, s);
     if (le != 0) return cuda_err(cudaError_t(le), "track kernel launch");
     TP_CUDA(cudaEventRecord(c->ev1, s));
     k_work_stats<<<sg, 256, 0, s>>>(c->alive0, d_lost, d_lt, d_le, n, prefix, nullptr, nullptr, nullptr, 0, a.nelem,
@@ -872,7 +899,7 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     S.h2d_bytes = h2d;
     S.d2h_bytes = d2h;
     S.block_size = block;
-    S.min_blocks = strict ? minb_track_strict(lc.minb) : minb_track_fast(lc.minb);
+    S.min_blocks = track_minb(build, lc.minb);
     S.grid = grid;
     S.launches = 3 + (lost_turn ? 0 : 1) + (lost_elem ? 0 : 1);
     S.schedule = schedule;
@@ -1088,7 +1115,8 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     cudaStream_t s = o.stream ? static_cast<cudaStream_t>(o.stream) : c->stream;
     const bool dev = o.device_pointers != 0;
     const bool exact = o.exact_hamiltonian != 0;
-    const bool strict = o.fp_contract == 0;
+    const TrackBuild build = track_build(o);
+    const bool strict = build != TB_FAST;
     int st = ensure_capacity(c, n);
     if (st != TP_OK) return st;
     double* d_coords = dev ? coords : c->coords;
@@ -1159,13 +1187,13 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     // Static tiles or pooled refill: the caller's choice, else tuned online.
     int64_t ph = 0;
     for (int32_t v = 0; v <= nvar; ++v) ph = ph * 1000003 + poff[v];
-    const uint64_t tkey = tune_key({n, nturns, int64_t(exact), int64_t(strict), block, ph, int64_t(b->table_words)});
+    const uint64_t tkey = tune_key({n, nturns, int64_t(exact), int64_t(build), block, ph, int64_t(b->table_words)});
     LaunchCand lc;
-    const bool tuning = pick_launch(&b->tune, nullptr, tkey, o, nturns, strict, a.rare != 0, &lc);
+    const bool tuning = pick_launch(&b->tune, nullptr, tkey, o, nturns, build, a.rare != 0, &lc);
     const int schedule = lc.sched;
     a.refill = schedule == 2 ? 1 : 0;
     int bps = 0;
-    int oerr = strict ? occupancy_track_strict(block, lc.minb, 0, &bps) : occupancy_track_fast(block, lc.minb, 0, &bps);
+    int oerr = track_occupancy(build, block, lc.minb, 0, &bps);
     if (oerr != 0 || bps <= 0) bps = 1;
     int grid = int(std::min<int64_t>(int64_t(c->sm_count) * bps, (tiles * 32 + block - 1) / block));
     grid = std::max(grid, 1);
@@ -1184,8 +1212,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
         k_alive_mask<<<sg, 256, 0, q>>>(d_lost, n, c->alive0, c->counters + 2);
         TP_CUDA(cudaGetLastError());
         if (timed) TP_CUDA(cudaEventRecord(c->ev0, q));
-        int le = strict ? launch_track_strict(a, grid, block, lc.minb, 0, q)
-                        : launch_track_fast(a, grid, block, lc.minb, 0, q);
+        int le = track_launch(build, a, grid, block, lc.minb, 0, q);
         if (le != 0) return cuda_err(cudaError_t(le), "batched track kernel launch");
         if (timed) TP_CUDA(cudaEventRecord(c->ev1, q));
         k_work_stats<<<sg, 256, 0, q>>>(c->alive0, d_lost, d_lt, d_le, n, d_pre, b->poff, d_pre_off, b->nelem_v, nvar,
@@ -1206,7 +1233,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
             u(d_coords), u(d_lost), u(d_lt), u(d_le), uint64_t(dev && lost_turn), uint64_t(dev && lost_elem),
             u(b->table), u(b->toff), u(b->poff), u(b->beti_v), u(b->nelem_v), u(b->mis), u(b->sched),
             u(b->sched_v), u(b->pool), u(b->prefix), u(b->prefix_off), u(d_pre),
-            uint64_t(uint32_t(nturns)), uint64_t(uint32_t(turn0)), uint64_t(exact), uint64_t(strict),
+            uint64_t(uint32_t(nturns)), uint64_t(uint32_t(turn0)), uint64_t(exact), uint64_t(build),
             uint64_t(a.refill), uint64_t(a.rare), dbits(a.limx), dbits(a.limy), dbits(a.beti),
             uint64_t(block), uint64_t(grid), uint64_t(sg), uint64_t(n), uint64_t(lc.minb)};
         for (int32_t v = 0; v <= nvar; ++v) key.push_back(uint64_t(poff[v]));
@@ -1263,7 +1290,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     S.h2d_bytes = h2d;
     S.d2h_bytes = d2h;
     S.block_size = block;
-    S.min_blocks = strict ? minb_track_strict(lc.minb) : minb_track_fast(lc.minb);
+    S.min_blocks = track_minb(build, lc.minb);
     S.grid = grid;
     S.launches = 3 + ((dev && lost_turn) ? 0 : 1) + ((dev && lost_elem) ? 0 : 1);
     S.schedule = schedule;

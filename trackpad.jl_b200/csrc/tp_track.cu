@@ -18,9 +18,13 @@
 // gives each thread one particle.  Batched launches hand out 32-particle
 // tiles of (variant, particles) and read each variant's table through L1.
 //
-// This file is compiled twice: with FMA contraction (TP_NS = fast) and
+// This file is compiled three times: with FMA contraction (TP_NS = fast),
 // without (-fmad=false, TP_NS = strict, bit-identical arithmetic to the
-// oracle except inside transcendental calls).
+// oracle), and without contraction with bounds checks (TP_NS = checked,
+// TP_BOUNDS_CHECK: every element-table record must lie inside its table or
+// turn block and every particle index below N, else the kernel sets DE_BOUNDS
+// in the error word and stops the warp's work instead of reading out of
+// bounds).
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -129,22 +133,50 @@ struct SchedView {
 };
 
 // Header of the record to use at `turn` (scheduled elements live in the
-// per-turn table).  Returns null when the turn is outside the schedule.
-__device__ __forceinline__ const double* resolve(const double* rec, RecHdr& h, const SchedView& sv, int turn) {
+// per-turn table).  Returns null when the turn is outside the schedule (and,
+// in the bounds-checked build, when the record does not fit its turn block,
+// with DE_BOUNDS set).
+__device__ __forceinline__ const double* resolve(const double* rec, RecHdr& h, const SchedView& sv, int turn,
+                                                 int32_t* err) {
+    (void)err;
     if (!(h.flags & RF_SCHEDULED)) return rec;
     int row = turn - sv.turn0;
     if (row < 0 || row >= sv.nturns) return nullptr;
-    const double* p = sv.p + int64_t(row) * sv.stride + h.aux;
+    const int32_t slot = h.aux;
+#ifdef TP_BOUNDS_CHECK
+    if (slot < 0 || slot + HDR_WORDS > sv.stride) {
+        atomicOr(err, DE_BOUNDS);
+        return nullptr;
+    }
+#endif
+    const double* p = sv.p + int64_t(row) * sv.stride + slot;
     h = *reinterpret_cast<const RecHdr*>(p);
+#ifdef TP_BOUNDS_CHECK
+    if (h.words < HDR_WORDS || slot + int32_t(h.words) > sv.stride) {
+        atomicOr(err, DE_BOUNDS);
+        return nullptr;
+    }
+#endif
     return p;
 }
+
+#ifdef TP_BOUNDS_CHECK
+// The walk over the element table left the table (a corrupt record length):
+// report it and end this warp's work (the condition is warp-uniform).
+__device__ __forceinline__ void table_overrun(const TrackArgs& a, bool& act, bool& more) {
+    if ((threadIdx.x & 31) == 0) atomicOr(a.err, DE_BOUNDS);
+    act = false;
+    more = false;
+}
+#endif
 
 // Track the particles of one warp through `nturns` turns of the table `tab`
 // (`nelem` records).  Slot state is per lane.  With REFILL, lanes take new
 // particles from `next_particle` at turn boundaries until it returns < 0.
 template <bool EXACT, bool REFILL, bool RARE, typename NextFn>
-__device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, double beti, const SchedView& sv,
-                         NextFn next_particle) {
+__device__ void run_warp(const TrackArgs& a, const double* tab, const double* tab_end, int nelem, double beti,
+                         const SchedView& sv, NextFn next_particle) {
+    (void)tab_end;  // read by the bounds-checked build only
     const double beta = 1.0 / beti;
     const double beta2 = beta * beta;
     const int lane = threadIdx.x & 31;
@@ -160,6 +192,12 @@ __device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, doubl
             unsigned need = __ballot_sync(0xffffffffu, !act);
             if (need == 0) break;
             int64_t j = next_particle(need, lane, more);
+#ifdef TP_BOUNDS_CHECK
+            if (j >= a.n) {
+                atomicOr(a.err, DE_BOUNDS);
+                j = -1;
+            }
+#endif
             if (!act && j >= 0) {
                 if (a.lost_flags[j] != 1) {
                     load_state(a.coords, a.n, j, s);
@@ -177,15 +215,27 @@ __device__ void run_warp(const TrackArgs& a, const double* tab, int nelem, doubl
         // One turn.
         const double* rec = tab;
         for (int e = 0; e < nelem; ++e) {
+#ifdef TP_BOUNDS_CHECK
+            if (rec + HDR_WORDS > tab_end) {
+                table_overrun(a, act, more);
+                break;
+            }
+#endif
             RecHdr h0 = *reinterpret_cast<const RecHdr*>(rec);
             const double* next = rec + h0.words;
+#ifdef TP_BOUNDS_CHECK
+            if (h0.words < HDR_WORDS || next > tab_end) {
+                table_overrun(a, act, more);
+                break;
+            }
+#endif
             // Every lane of this warp empty: skip the rest of the turn.  (The vote
             // at every element also reconverges the warp after divergent maps;
             // voting every 16 elements measured 4% slower on the DBA ring.)
             if (__ballot_sync(0xffffffffu, act) == 0) break;
             if (act) {
                 RecHdr h = h0;
-                const double* r = resolve(rec, h, sv, a.turn0 + t);
+                const double* r = resolve(rec, h, sv, a.turn0 + t, a.err);
                 if (r == nullptr) {
                     atomicOr(a.err, DE_SCHED_RANGE);
                     act = false;
@@ -243,14 +293,14 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) track_single(TrackArgs a) {
             unsigned long long j = base + __popc(need & ((1u << lane) - 1u));
             return j < (unsigned long long)a.n ? int64_t(j) : -1;
         };
-        run_warp<EXACT, true, RARE>(a, tab, a.nelem, a.beti, sv, next);
+        run_warp<EXACT, true, RARE>(a, tab, tab + a.table_words, a.nelem, a.beti, sv, next);
     } else {
         const int64_t gid = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
         auto next = [&](unsigned need, int lane, bool& more) -> int64_t {
             more = false;
             return gid < a.n ? gid : -1;
         };
-        run_warp<EXACT, false, RARE>(a, tab, a.nelem, a.beti, sv, next);
+        run_warp<EXACT, false, RARE>(a, tab, tab + a.table_words, a.nelem, a.beti, sv, next);
     }
 }
 
@@ -306,7 +356,8 @@ __global__ void __launch_bounds__(kMaxBlock, MINB) track_batched(TrackArgs a, co
             sv.turn0 = int32_t(a.sched_v[4 * v + 2]);
             sv.nturns = int32_t(a.sched_v[4 * v + 3]);
         }
-        run_warp<EXACT, REFILL, RARE>(a, a.table + a.toff[v], a.nelem_v[v], a.beti_v[v], sv, next);
+        run_warp<EXACT, REFILL, RARE>(a, a.table + a.toff[v], a.table + a.toff[v + 1], a.nelem_v[v], a.beti_v[v], sv,
+                                      next);
     }
 }
 

@@ -39,6 +39,7 @@ struct TpOpts
     size::Int32; exact_hamiltonian::Int32; device_pointers::Int32; fp_contract::Int32
     block_size::Int32; min_blocks::Int32; schedule::Int32; table_in_smem::Int32
     aperture_x::Float64; aperture_y::Float64; stream::Ptr{Cvoid}
+    bounds_check::Int32; reserved0::Int32
 end
 
 struct TpLossSpec
@@ -192,7 +193,7 @@ end
 
 opts(device::Bool; aperture = 0.0) =
     TpOpts(Int32(sizeof(TpOpts)), 1, device ? 1 : 0, 0, 0, 0, 0, 0, aperture, aperture,
-           device ? Ptr{Cvoid}(CUDA.stream().handle) : C_NULL)
+           device ? Ptr{Cvoid}(CUDA.stream().handle) : C_NULL, 0, 0)
 
 """ringpass! on the GPU for device arrays: coords is N x 6 (column-major, as on the CPU)."""
 function TrackPad.ringpass!(coords::CuMatrix{Float64}, lat::Lattice, beam::Beam{Float64},

@@ -293,7 +293,7 @@ TABLE_IN_SMEM = False
 
 
 def _opts(aperture, exact, contract, device, block_size=0, schedule=0, stream=None, device_index=None,
-          min_blocks=0):
+          min_blocks=0, bounds_check=False):
     """tp_opts of a call.  With device arrays and no stream given, the call runs
     on PyTorch's current stream of that device, so the kernels follow the work
     that wrote the inputs there; PyTorch's default stream has handle 0, which
@@ -310,6 +310,7 @@ def _opts(aperture, exact, contract, device, block_size=0, schedule=0, stream=No
     o.block_size = int(block_size)
     o.schedule = int(schedule)
     o.min_blocks = int(min_blocks)
+    o.bounds_check = 1 if bounds_check else 0
     if aperture is not None:
         ax, ay = (aperture, aperture) if np.isscalar(aperture) else aperture
         o.aperture_x, o.aperture_y = float(ax), float(ay)
@@ -389,7 +390,7 @@ class _Buffers:
 
 def ringpass_(coords, lat, beam, lost_flags, nturns, *, time=0.0, dt_turn=0.0, turn=0, aperture=None,
               lost_turn=None, lost_elem=None, exact=True, contract=False, block_size=0, schedule=0, stream=None,
-              min_blocks=0):
+              min_blocks=0, bounds_check=False):
     """ringpass!(coords, lat, beam, lost_flags, nturns; time, dt_turn, turn) on the GPU.
 
     Extra keywords: `aperture` (half width, or (ax, ay)) adds the rectangular
@@ -399,7 +400,9 @@ def ringpass_(coords, lat, beam, lost_flags, nturns, *, time=0.0, dt_turn=0.0, t
     kernel built with FMA contraction (faster; its rounding differs from the
     reference's operation order); `schedule` (1 static, 2 lane refill) and
     `min_blocks` (kernel instance sized for 7, 6 or 5 resident blocks per SM)
-    fix what the autotuner otherwise picks (0).
+    fix what the autotuner otherwise picks (0); `bounds_check=True` runs the
+    kernels that check every element-table record and particle index before
+    reading it (a violation raises with TP_EDEVICE).
     """
     if not isinstance(lat, Lattice):
         lat = Lattice(lat)
@@ -410,7 +413,7 @@ def ringpass_(coords, lat, beam, lost_flags, nturns, *, time=0.0, dt_turn=0.0, t
     lat.set_schedule(time, dt_turn, turn, max(nturns, 1))
     dev = b.device_index if b.device else None
     o = _opts(aperture, exact, contract, b.device, block_size, schedule, stream, device_index=dev,
-              min_blocks=min_blocks)
+              min_blocks=min_blocks, bounds_check=bounds_check)
     st = _abi.lib().tp_ringpass(context(dev), lat.handle, b.coords, b.n, b.lost, b.lost_turn, b.lost_elem,
                                 C.c_double(beti(beam)), nturns, C.c_double(time), C.c_double(dt_turn), int(turn),
                                 C.byref(o))
@@ -448,7 +451,7 @@ class Batch:
 
     def ringpass_(self, coords, poff, betis, lost_flags, nturns, *, time=0.0, dt_turn=0.0, turn=0, aperture=None,
                   lost_turn=None, lost_elem=None, exact=True, contract=False, use_graph=True, block_size=0,
-                  schedule=0, stream=None, min_blocks=0):
+                  schedule=0, stream=None, min_blocks=0, bounds_check=False):
         """ringpass! of every variant in one launch; variant v owns particles
         poff[v]..poff[v+1].  Time-dependent variants are evaluated per turn."""
         b = _Buffers(coords, lost_flags, lost_turn, lost_elem)
@@ -461,7 +464,8 @@ class Batch:
         if poff[-1] != b.n:
             raise ValueError("poff[-1] must equal the number of particles")
         o = _opts(aperture, exact, contract, b.device, block_size, schedule, stream,
-                  device_index=b.device_index if b.device else None, min_blocks=min_blocks)
+                  device_index=b.device_index if b.device else None, min_blocks=min_blocks,
+                  bounds_check=bounds_check)
         st = _abi.lib().tp_ringpass_batched(context(self.device), self._handle, b.coords,
                                             poff.ctypes.data_as(C.c_void_p), b.lost, b.lost_turn, b.lost_elem,
                                             betis.ctypes.data_as(C.c_void_p), int(nturns), C.c_double(0.0),
