@@ -96,8 +96,8 @@ def adjoint_gpu(rank, world):
     c0 = np.asfortranarray(np.concatenate([W.gaussian(2000, seed=6), W.da_grid(8, 8, half=0.019)]))
     lo, hi = tp.sharding.particle_shard(len(c0), rank, world)
     loss, grad = tp.sharding.distributed_ringpass_adjoint(np.asfortranarray(c0[lo:hi]), lat, beam, None, 8, params,
-                                                          sigma=1e-4, lost_weight=1e3, aperture=0.02)
-    rloss, rgrad = tp.ringpass_adjoint(c0, lat, beam, None, 8, params, sigma=1e-4, lost_weight=1e3, aperture=0.02)[:2]
+                                                          checkpoint_every=1, sigma=1e-4, lost_weight=1e3, aperture=0.02)
+    rloss, rgrad = tp.ringpass_adjoint(c0, lat, beam, None, 8, params, checkpoint_every=1, sigma=1e-4, lost_weight=1e3, aperture=0.02)[:2]
     return {"rank": rank, "loss": loss, "ref_loss": rloss,
             "grad_err": float(np.abs(grad - rgrad).max() / np.abs(rgrad).max())}
 

@@ -57,7 +57,7 @@ def test_adjoint_dba_cells_match_dual_oracle():
     lat, beam = W.dba_ring(cells=2), W.dba_beam()
     params = W.magnet_indices(lat)
     c0 = W.gaussian(256, seed=21)
-    loss, g, cout, lout = tp.ringpass_adjoint(c0, lat, beam, None, 8, params, sigma=SIGMA, lost_weight=LW,
+    loss, g, cout, lout = tp.ringpass_adjoint(c0, lat, beam, None, 8, params, checkpoint_every=1, sigma=SIGMA, lost_weight=LW,
                                               aperture=0.02, return_state=True)
     st = tp.adjoint_stats()
     rloss, rg, rsurv = oracle_grad(lat, c0, beam, 8, params, 0.02)
@@ -171,7 +171,7 @@ def test_adjoint_every_reverse_map():
     lat, beam = mixed_lattice(), tp.Beam(3.5e9)
     params = [2, 4, 6, 8]
     c0 = W.gaussian(128, seed=25)
-    loss, g = tp.ringpass_adjoint(c0, lat, beam, None, 4, params, sigma=SIGMA, aperture=0.05)
+    loss, g = tp.ringpass_adjoint(c0, lat, beam, None, 4, params, checkpoint_every=1, sigma=SIGMA, aperture=0.05)
     rloss, rg, _ = oracle_grad(lat, c0, beam, 4, params, 0.05)
     assert abs(loss - rloss) <= 1e-12 * abs(rloss)
     assert_grad_close(g, rg)
@@ -230,10 +230,10 @@ def test_batched_adjoint_equals_lattice_by_lattice():
     coords = np.asfortranarray(np.concatenate([W.gaussian(n, seed=30 + i) for i, n in enumerate(counts)]))
     params = [W.magnet_indices(v) for v, _ in variants]
     loss, grads = batch.ringpass_adjoint(coords, poff, np.full(len(counts), tp.beti(beam)), None, 5, params,
-                                         sigma=SIGMA, aperture=0.02)
+                                         checkpoint_every=1, sigma=SIGMA, aperture=0.02)
     for i, (lat, n) in enumerate(variants):
         l1, g1 = tp.ringpass_adjoint(np.asfortranarray(coords[poff[i]:poff[i + 1]]), lat, beam, None, 5, params[i],
-                                     sigma=SIGMA, aperture=0.02)
+                                     checkpoint_every=1, sigma=SIGMA, aperture=0.02)
         assert loss[i] == l1
         assert np.array_equal(grads[i], g1)
 
@@ -252,10 +252,10 @@ def test_batched_time_dependent_adjoint():
     coords = np.asfortranarray(np.concatenate([W.gaussian(n, seed=50 + i) for i, n in enumerate(counts)]))
     params = [W.magnet_indices(v) for v, _ in variants]
     loss, grads = batch.ringpass_adjoint(coords, poff, np.full(len(counts), tp.beti(beam)), None, nt, params,
-                                         sigma=SIGMA, aperture=0.02, checkpoint_every=5)
+                                         checkpoint_every=1, sigma=SIGMA, aperture=0.02, checkpoint_every=5)
     for i, lat in enumerate(lats):
         c = np.asfortranarray(coords[poff[i]:poff[i + 1]])
-        l1, g1 = tp.ringpass_adjoint(c, lat, beam, None, nt, params[i], sigma=SIGMA, aperture=0.02,
+        l1, g1 = tp.ringpass_adjoint(c, lat, beam, None, nt, params[i], checkpoint_every=1, sigma=SIGMA, aperture=0.02,
                                      checkpoint_every=5)
         assert loss[i] == l1 and np.array_equal(grads[i], g1)
     # variant 0 against the oracle with the same per-turn values

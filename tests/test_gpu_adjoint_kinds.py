@@ -107,7 +107,7 @@ def test_adjoint_through_every_kind_matches_dual_oracle():
     lat, beam = kinds_lattice(strong=False), tp.Beam(E0)
     params = [i for i, e in enumerate(lat.elements) if e.kind == "QUADRUPOLE"]
     c0 = W.gaussian(192, seed=45, sigma=BEAM_SIGMA)
-    loss, g = tp.ringpass_adjoint(c0, lat, beam, None, 4, params, sigma=SIGMA, lost_weight=LW, aperture=0.05)[:2]
+    loss, g = tp.ringpass_adjoint(c0, lat, beam, None, 4, params, checkpoint_every=1, sigma=SIGMA, lost_weight=LW, aperture=0.05)[:2]
     rloss, rg, rsurv = oracle_grad(lat, c0, beam, 4, params, 0.05)
     assert rsurv > 100
     assert abs(loss - rloss) <= 1e-12 * abs(rloss)
@@ -149,7 +149,7 @@ def test_adjoint_with_misalignment_rows_matches_dual_oracle():
     assert lat.pack()[3] > 0  # misalignment rows present
     params = W.magnet_indices(lat)
     c0 = W.gaussian(256, seed=47)
-    loss, g = tp.ringpass_adjoint(c0, lat, beam, None, 6, params, sigma=SIGMA, lost_weight=LW, aperture=0.02)[:2]
+    loss, g = tp.ringpass_adjoint(c0, lat, beam, None, 6, params, checkpoint_every=1, sigma=SIGMA, lost_weight=LW, aperture=0.02)[:2]
     rloss, rg, _ = oracle_grad(lat, c0, beam, 6, params, 0.02)
     assert abs(loss - rloss) <= 1e-12 * abs(rloss)
     assert_grad_close(g, rg)

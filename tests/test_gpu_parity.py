@@ -447,7 +447,7 @@ def test_table_in_shared_memory_or_l1_gives_the_same_bits():
             c = np.asfortranarray(c0.copy())
             lost = np.zeros(len(c), np.int64)
             tp.ringpass_(c, lat, beam, lost, 5, aperture=0.02)
-            loss, g = tp.ringpass_adjoint(c0, lat, beam, None, 3, params, sigma=1e-4, aperture=0.02)[:2]
+            loss, g = tp.ringpass_adjoint(c0, lat, beam, None, 3, params, checkpoint_every=1, sigma=1e-4, aperture=0.02)[:2]
             out.append((c, lost, loss, g))
         finally:
             tp.tracking.TABLE_IN_SMEM = False

@@ -329,12 +329,17 @@ __device__ __forceinline__ bool is_normal(double v) {
     return av >= 2.2250738585072014e-308 && av <= 1.7976931348623157e308;
 }
 
+// The IEEE division of div_rcp's rare out-of-range case, out of line: the
+// kernels are limited by instruction fetch, and three inlined divisions in the
+// exact-bend body loop cost more there than the call on the rare path.
+static __device__ __noinline__ double div_ool(double a, double b) { return a / b; }
+
 __device__ __forceinline__ double div_rcp(double a, double b, double y) {
     double q = __dmul_rn(a, y);
     double r = fma(-q, b, a);
     double q1 = fma(r, y, q);
     double aq = fabs(q);
-    if (!(aq > 1e-280 && aq < 1e280)) q1 = a / b;
+    if (!(aq > 1e-280 && aq < 1e280)) q1 = div_ool(a, b);
     return q1;
 }
 
