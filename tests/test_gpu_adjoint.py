@@ -252,10 +252,10 @@ def test_batched_time_dependent_adjoint():
     coords = np.asfortranarray(np.concatenate([W.gaussian(n, seed=50 + i) for i, n in enumerate(counts)]))
     params = [W.magnet_indices(v) for v, _ in variants]
     loss, grads = batch.ringpass_adjoint(coords, poff, np.full(len(counts), tp.beti(beam)), None, nt, params,
-                                         checkpoint_every=1, sigma=SIGMA, aperture=0.02, checkpoint_every=5)
+                                         sigma=SIGMA, aperture=0.02, checkpoint_every=5)
     for i, lat in enumerate(lats):
         c = np.asfortranarray(coords[poff[i]:poff[i + 1]])
-        l1, g1 = tp.ringpass_adjoint(c, lat, beam, None, nt, params[i], checkpoint_every=1, sigma=SIGMA, aperture=0.02,
+        l1, g1 = tp.ringpass_adjoint(c, lat, beam, None, nt, params[i], sigma=SIGMA, aperture=0.02,
                                      checkpoint_every=5)
         assert loss[i] == l1 and np.array_equal(grads[i], g1)
     # variant 0 against the oracle with the same per-turn values
