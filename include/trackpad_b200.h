@@ -232,6 +232,9 @@ typedef struct tp_stats {
     int32_t launches;          /* kernels this library launched in the call      */
     int32_t schedule;          /* 1 = static, 2 = lane refill                      */
     int32_t fp_contract;
+    int32_t refill_fold;       /* batched pooled refill: variant particles per warp
+                                  tile / 32 (1 = one tile per 32 particles)       */
+    int32_t bounds_check;      /* 1: the bounds-checked kernels ran               */
 } tp_stats;
 
 /* ------------------------------------------------------------------------- */

@@ -487,3 +487,32 @@ def test_bounds_checked_kernels_give_the_same_bits():
                         bounds_check=bc)
         bo.append((cb, lb))
     assert np.array_equal(bo[0][0], bo[1][0]) and np.array_equal(bo[0][1], bo[1][1])
+
+
+def test_batched_refill_folds_are_tuned_and_keep_the_bits():
+    """Pooled refill with fewer warps per variant (1/2 and 1/4 of the 32-particle
+    tiles, each warp refilling from the variant's pool more often): the tuner
+    times folds 1, 2, 4 on the first calls and keeps one; every call gives the
+    same bits."""
+    variants = W.dba_variants(nvar=5, seed=16, n_base=300, cells_range=(2, 5))
+    counts = [n for _, n in variants]
+    poff = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+    coords = np.asfortranarray(np.concatenate([np.concatenate([W.gaussian(n - n // 4, seed=110 + i),
+                                                               W.da_grid(1, n // 4, half=0.019)])
+                                               for i, n in enumerate(counts)]))
+    batch = tp.Batch([v for v, _ in variants])
+    beam = W.dba_beam()
+    seen, outs = [], []
+    for _ in range(5):
+        c = coords.copy(order="F")
+        l = np.zeros(len(c), np.int64)
+        lt = np.full(len(c), -1, np.int32)
+        batch.ringpass_(c, poff, np.full(5, tp.beti(beam)), l, 10, aperture=0.02, lost_turn=lt, schedule=2,
+                        min_blocks=7, use_graph=True)
+        seen.append(tp.last_stats()["refill_fold"])
+        outs.append((c, l, lt))
+    assert seen[:3] == [1, 2, 4] and seen[3] == seen[4] and seen[3] in (1, 2, 4)
+    for o in outs[1:]:
+        for a, b in zip(o, outs[0]):
+            assert np.array_equal(a, b)
+    assert 0 < outs[0][1].sum() < len(coords)

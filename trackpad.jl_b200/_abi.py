@@ -73,7 +73,8 @@ class TpStats(C.Structure):
         ("particles", C.c_int64), ("survivors", C.c_int64), ("element_passes", C.c_int64), ("units", C.c_double),
         ("flops", C.c_double), ("kernel_ms", C.c_double), ("total_ms", C.c_double), ("h2d_bytes", C.c_int64),
         ("d2h_bytes", C.c_int64), ("block_size", C.c_int32), ("min_blocks", C.c_int32), ("grid", C.c_int32),
-        ("launches", C.c_int32), ("schedule", C.c_int32), ("fp_contract", C.c_int32),
+        ("launches", C.c_int32), ("schedule", C.c_int32), ("fp_contract", C.c_int32), ("refill_fold", C.c_int32),
+        ("bounds_check", C.c_int32),
     ]
 
 

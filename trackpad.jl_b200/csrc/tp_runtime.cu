@@ -56,6 +56,7 @@ constexpr int kMaxDevices = 16;
 // fastest candidate.  What the caller fixes in tp_opts is not tuned.
 struct LaunchCand {
     int sched = 1, minb = 7;
+    int fold = 1;  // batched pooled refill: warps per variant = tiles / fold (more refills per warp)
 };
 
 struct LaunchTune {
@@ -63,7 +64,7 @@ struct LaunchTune {
     LaunchCand cand[6];
     float ms[6] = {};
     int ncand = 0, ntried = 0;
-    bool staged = false;  // the resident-block candidates have been appended
+    int stage = 0;       // 0: schedules, 1: resident blocks, 2: batched refill folds, 3: settled
     LaunchCand best;
 };
 
@@ -78,29 +79,43 @@ uint64_t tune_key(std::initializer_list<int64_t> parts) {
     return h | 1ull;
 }
 
+int tune_argmin(const LaunchTune& t) {
+    int bi = 0;
+    for (int k = 1; k < t.ntried; ++k)
+        if (t.ms[k] < t.ms[bi]) bi = k;
+    return bi;
+}
+
 // The candidate for this call.  fixed_sched / fixed_minb: the caller's choice
 // (0: tuned).  minbs[0..nminb): the resident-block counts the kernel build
-// carries, the default first.  *trial is set when the call is a timing trial.
+// carries, the default first.  folds: whether batched refill folds are tried.
+// *trial is set when the call is a timing trial.
 LaunchCand tune_pick(LaunchTune& t, uint64_t key, int fixed_sched, int fixed_minb, const int* minbs, int nminb,
-                     bool* trial) {
+                     bool folds, bool* trial) {
     if (t.key != key) {
         t = LaunchTune{};
         t.key = key;
         const int m0 = fixed_minb ? fixed_minb : minbs[0];
         if (fixed_sched) {
-            t.cand[t.ncand++] = {fixed_sched, m0};
+            t.cand[t.ncand++] = {fixed_sched, m0, 1};
         } else {
-            t.cand[t.ncand++] = {1, m0};
-            t.cand[t.ncand++] = {2, m0};
+            t.cand[t.ncand++] = {1, m0, 1};
+            t.cand[t.ncand++] = {2, m0, 1};
         }
-        t.staged = fixed_minb != 0 || nminb <= 1;
     }
-    if (t.ntried == t.ncand && !t.staged) {
-        int bi = 0;
-        for (int k = 1; k < t.ntried; ++k)
-            if (t.ms[k] < t.ms[bi]) bi = k;
-        for (int k = 1; k < nminb && t.ncand < 6; ++k) t.cand[t.ncand++] = {t.cand[bi].sched, minbs[k]};
-        t.staged = true;
+    while (t.ntried == t.ncand && t.stage < 3) {
+        const LaunchCand b = t.cand[tune_argmin(t)];
+        if (t.stage == 0 && !fixed_minb && nminb > 1) {
+            for (int k = 1; k < nminb && t.ncand < 6; ++k) t.cand[t.ncand++] = {b.sched, minbs[k], 1};
+            t.stage = 1;
+        } else if (t.stage <= 1 && folds && b.sched == 2) {
+            for (int f : {2, 4})
+                if (t.ncand < 6) t.cand[t.ncand++] = {2, b.minb, f};
+            t.stage = 2;
+        } else {
+            t.best = b;
+            t.stage = 3;
+        }
     }
     if (t.ntried < t.ncand) {
         *trial = true;
@@ -112,19 +127,11 @@ LaunchCand tune_pick(LaunchTune& t, uint64_t key, int fixed_sched, int fixed_min
 
 void tune_record(LaunchTune& t, uint64_t key, LaunchCand c, float ms) {
     if (t.key != key || t.ntried >= t.ncand) return;
-    if (t.cand[t.ntried].sched != c.sched || t.cand[t.ntried].minb != c.minb) return;
+    const LaunchCand& e = t.cand[t.ntried];
+    if (e.sched != c.sched || e.minb != c.minb || e.fold != c.fold) return;
     t.ms[t.ntried++] = ms;
-    if (t.ntried == t.ncand && t.staged) {
-        int bi = 0;
-        for (int k = 1; k < t.ntried; ++k)
-            if (t.ms[k] < t.ms[bi]) bi = k;
-        t.best = t.cand[bi];
-    }
 }
 
-// The launch configuration of one tracking call: the caller's choices, else
-// the tuner's (multi-turn tracks only; single passes run static at the
-// default).  Returns whether the call is a timing trial.
 // The three builds of the tracking kernels (tp_track.cu): with FMA
 // contraction, without, and without with bounds checks.
 enum TrackBuild { TB_FAST = 0, TB_STRICT = 1, TB_CHECKED = 2 };
@@ -153,23 +160,25 @@ int track_minb(TrackBuild b, int minb) {
 }
 
 bool pick_launch(LaunchTune* tu, std::mutex* mu, uint64_t key, const tp_opts& o, int nturns, TrackBuild build,
-                 bool rare, LaunchCand* out) {
+                 bool rare, bool batched, LaunchCand* out) {
     int minbs[3] = {7, 6, 5};
     int nminb = 1;
     if (!rare && track_minb(build, 5) == 5 && track_minb(build, 6) == 6) nminb = 3;
     const int fixed_minb = o.min_blocks > 0 ? track_minb(build, o.min_blocks) : 0;
     const int fixed_sched = o.schedule == 1 || o.schedule == 2 ? o.schedule : 0;
-    if (nturns <= 1 || (fixed_sched && (fixed_minb || nminb == 1))) {
+    const bool folds = batched && fixed_sched != 1;
+    if (nturns <= 1 || (fixed_sched && (fixed_minb || nminb == 1) && !folds)) {
         out->sched = fixed_sched ? fixed_sched : 1;
         out->minb = fixed_minb ? fixed_minb : minbs[0];
+        out->fold = 1;
         return false;
     }
     bool trial = false;
     if (mu) {
         std::lock_guard<std::mutex> g(*mu);
-        *out = tune_pick(*tu, key, fixed_sched, fixed_minb, minbs, nminb, &trial);
+        *out = tune_pick(*tu, key, fixed_sched, fixed_minb, minbs, nminb, folds, &trial);
     } else {
-        *out = tune_pick(*tu, key, fixed_sched, fixed_minb, minbs, nminb, &trial);
+        *out = tune_pick(*tu, key, fixed_sched, fixed_minb, minbs, nminb, folds, &trial);
     }
     return trial;
 }
@@ -843,7 +852,8 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     const uint64_t tkey = tune_key({n, nturns, int64_t(exact), int64_t(build), block, int64_t(L->version),
                                     int64_t(L->program.size()), int64_t(smem)});
     LaunchCand lc;
-    const bool tuning = pick_launch(&L->dev[c->device].tune, &L->mu, tkey, o, nturns, build, a.rare != 0, &lc);
+    const bool tuning = pick_launch(&L->dev[c->device].tune, &L->mu, tkey, o, nturns, build, a.rare != 0, false,
+                                    &lc);
     const int schedule = lc.sched;
     a.refill = schedule == 2 ? 1 : 0;
     int bps = 0;
@@ -904,6 +914,8 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     S.launches = 3 + (lost_turn ? 0 : 1) + (lost_elem ? 0 : 1);
     S.schedule = schedule;
     S.fp_contract = strict ? 0 : 1;
+    S.refill_fold = 1;
+    S.bounds_check = build == TB_CHECKED ? 1 : 0;
     return TP_OK;
 }
 
@@ -1131,28 +1143,6 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
         if (lost_turn) { TP_CUDA(cudaMemcpyAsync(d_lt, lost_turn, size_t(n) * 4, cudaMemcpyHostToDevice, s)); h2d += n * 4; }
         if (lost_elem) { TP_CUDA(cudaMemcpyAsync(d_le, lost_elem, size_t(n) * 4, cudaMemcpyHostToDevice, s)); h2d += n * 4; }
     }
-    // Per-variant offsets, betas, tile offsets and flop prefix tables.  Tiles
-    // are handed out longest first: the variants with the most elements (the
-    // longest 32-particle loads) come first, so that short loads fill the end
-    // of the launch.  Layout: toff[nvar+1], tile offsets in that order
-    // [nvar+1], the order itself [nvar].
-    std::vector<int32_t> order(static_cast<size_t>(nvar));
-    for (int32_t v = 0; v < nvar; ++v) order[size_t(v)] = v;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int32_t x, int32_t y) { return b->h_nelem[size_t(x)] > b->h_nelem[size_t(y)]; });
-    std::vector<int64_t> offs(3 * (size_t(nvar) + 1));
-    for (int32_t v = 0; v <= nvar; ++v) offs[size_t(v)] = b->h_toff[size_t(v)];
-    int64_t tiles = 0;
-    for (int32_t k = 0; k < nvar; ++k) {
-        const int32_t v = order[size_t(k)];
-        offs[size_t(nvar) + 1 + size_t(k)] = tiles;
-        offs[2 * (size_t(nvar) + 1) + size_t(k)] = v;
-        tiles += (poff[v + 1] - poff[v] + 31) / 32;
-    }
-    offs[2 * (size_t(nvar) + 1) - 1] = tiles;
-    TP_CUDA(cudaMemcpyAsync(b->toff, offs.data(), offs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s));
-    TP_CUDA(cudaMemcpyAsync(b->beti_v, beti, size_t(nvar) * sizeof(double), cudaMemcpyHostToDevice, s));
-    TP_CUDA(cudaMemcpyAsync(b->poff, poff, (size_t(nvar) + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
     const double* d_pre = b->prefix + (exact ? 0 : b->prefix_words);
     const int64_t* d_pre_off = b->prefix_off;
 
@@ -1189,9 +1179,34 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     for (int32_t v = 0; v <= nvar; ++v) ph = ph * 1000003 + poff[v];
     const uint64_t tkey = tune_key({n, nturns, int64_t(exact), int64_t(build), block, ph, int64_t(b->table_words)});
     LaunchCand lc;
-    const bool tuning = pick_launch(&b->tune, nullptr, tkey, o, nturns, build, a.rare != 0, &lc);
+    const bool tuning = pick_launch(&b->tune, nullptr, tkey, o, nturns, build, a.rare != 0, true, &lc);
     const int schedule = lc.sched;
     a.refill = schedule == 2 ? 1 : 0;
+    const int fold = a.refill ? std::max(1, lc.fold) : 1;
+    // Per-variant offsets, betas, tile offsets and flop prefix tables.  Tiles
+    // are handed out longest first: the variants with the most elements (the
+    // longest 32-particle loads) come first, so that short loads fill the end
+    // of the launch.  With pooled refill, `fold` > 1 hands out 1/fold as many
+    // tiles per variant: fewer warps per variant, each refilling its lanes
+    // from the variant's pool more often.  Layout: toff[nvar+1], tile offsets in that order
+    // [nvar+1], the order itself [nvar].
+    std::vector<int32_t> order(static_cast<size_t>(nvar));
+    for (int32_t v = 0; v < nvar; ++v) order[size_t(v)] = v;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t x, int32_t y) { return b->h_nelem[size_t(x)] > b->h_nelem[size_t(y)]; });
+    std::vector<int64_t> offs(3 * (size_t(nvar) + 1));
+    for (int32_t v = 0; v <= nvar; ++v) offs[size_t(v)] = b->h_toff[size_t(v)];
+    int64_t tiles = 0;
+    for (int32_t k = 0; k < nvar; ++k) {
+        const int32_t v = order[size_t(k)];
+        offs[size_t(nvar) + 1 + size_t(k)] = tiles;
+        offs[2 * (size_t(nvar) + 1) + size_t(k)] = v;
+        tiles += (poff[v + 1] - poff[v] + 32 * fold - 1) / (32 * fold);
+    }
+    offs[2 * (size_t(nvar) + 1) - 1] = tiles;
+    TP_CUDA(cudaMemcpyAsync(b->toff, offs.data(), offs.size() * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+    TP_CUDA(cudaMemcpyAsync(b->beti_v, beti, size_t(nvar) * sizeof(double), cudaMemcpyHostToDevice, s));
+    TP_CUDA(cudaMemcpyAsync(b->poff, poff, (size_t(nvar) + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
     int bps = 0;
     int oerr = track_occupancy(build, block, lc.minb, 0, &bps);
     if (oerr != 0 || bps <= 0) bps = 1;
@@ -1235,7 +1250,7 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
             u(b->sched_v), u(b->pool), u(b->prefix), u(b->prefix_off), u(d_pre),
             uint64_t(uint32_t(nturns)), uint64_t(uint32_t(turn0)), uint64_t(exact), uint64_t(build),
             uint64_t(a.refill), uint64_t(a.rare), dbits(a.limx), dbits(a.limy), dbits(a.beti),
-            uint64_t(block), uint64_t(grid), uint64_t(sg), uint64_t(n), uint64_t(lc.minb)};
+            uint64_t(block), uint64_t(grid), uint64_t(sg), uint64_t(n), uint64_t(lc.minb), uint64_t(fold)};
         for (int32_t v = 0; v <= nvar; ++v) key.push_back(uint64_t(poff[v]));
         if (!b->graph || b->g_key != key) {
             if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
@@ -1295,6 +1310,8 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     S.launches = 3 + ((dev && lost_turn) ? 0 : 1) + ((dev && lost_elem) ? 0 : 1);
     S.schedule = schedule;
     S.fp_contract = strict ? 0 : 1;
+    S.refill_fold = fold;
+    S.bounds_check = build == TB_CHECKED ? 1 : 0;
     return TP_OK;
 }
 
