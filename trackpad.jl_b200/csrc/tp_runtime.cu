@@ -850,7 +850,7 @@ static int track_common(tp_ctx* c, tp_lattice* L, double* coords, int64_t n, int
     const TrackBuild build = track_build(o);
     const bool strict = build != TB_FAST;
     const uint64_t tkey = tune_key({n, nturns, int64_t(exact), int64_t(build), block, int64_t(L->version),
-                                    int64_t(L->program.size()), int64_t(smem)});
+                                    int64_t(L->program.size()), int64_t(smem), o.schedule, o.min_blocks});
     LaunchCand lc;
     const bool tuning = pick_launch(&L->dev[c->device].tune, &L->mu, tkey, o, nturns, build, a.rare != 0, false,
                                     &lc);
@@ -1177,7 +1177,8 @@ TP_API int tp_ringpass_batched(tp_ctx* c, tp_batch* b, double* coords, const int
     // Static tiles or pooled refill: the caller's choice, else tuned online.
     int64_t ph = 0;
     for (int32_t v = 0; v <= nvar; ++v) ph = ph * 1000003 + poff[v];
-    const uint64_t tkey = tune_key({n, nturns, int64_t(exact), int64_t(build), block, ph, int64_t(b->table_words)});
+    const uint64_t tkey = tune_key({n, nturns, int64_t(exact), int64_t(build), block, ph, int64_t(b->table_words),
+                                    o.schedule, o.min_blocks});
     LaunchCand lc;
     const bool tuning = pick_launch(&b->tune, nullptr, tkey, o, nturns, build, a.rare != 0, true, &lc);
     const int schedule = lc.sched;
