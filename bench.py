@@ -44,10 +44,10 @@ SIGMA_LOSS = 1e-4      # sigma_x of the beam-size loss
 LOST_WEIGHT = 1e3
 
 # DRAM bytes per particle of one tracking launch: ncu capture of track_single on
-# the DBA ring, 135,168 particles (one full wave) x 10 turns, 1.407 GB read +
-# written, almost all of it the write-back of spilled stack lines.  Scaled by
-# the launch's particle count.
-DRAM_BYTES_PER_PARTICLE = 1.407376e9 / 135168
+# the DBA ring, 135,168 particles (one full wave) x 10 turns, 1.324 GB read +
+# written (dram__bytes.sum.per_second x gpu__time_duration), almost all of it
+# the write-back of spilled stack lines.  Scaled by the launch's particle count.
+DRAM_BYTES_PER_PARTICLE = 1.3236e9 / 135168
 
 
 def parse():

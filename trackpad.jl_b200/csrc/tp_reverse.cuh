@@ -153,24 +153,25 @@ __device__ __noinline__ void rev_multipole(P6& s, L6& l, const double* w, int ns
     make_cache(s, beti, c);  // delta is unchanged by the element
     // Backwards, the first D(L1) of a step (j = 0) and the last D(L1) of the
     // step before it (j = 3) follow each other with no kick between: px, py and
-    // delta are the same, so the second reuses the first's pz2 and N (the same
-    // bits).  The sweep runs on survivors only, where pz2 > 0.
-    double pz2 = 1.0, N = 0.0;
+    // delta are the same, so the second reuses the first's N (the same bits).
+    // The pull-back's N / pz2 = L / pz2^(3/2) is N^3 / L^2, with 1/L^2 once per
+    // element: no division per drift (a few ulps, which the gradient's
+    // tolerance leaves room for).  The sweep runs on survivors only, pz2 > 0.
+    // (a zero length has N = 0 and no pull-back term)
+    const double iL1sq = L1 * L1 > 0.0 ? 1.0 / (L1 * L1) : 0.0, iL2sq = L2 * L2 > 0.0 ? 1.0 / (L2 * L2) : 0.0;
+    double N = 0.0;
 #pragma unroll 1
     for (int k = 4 * nsteps - 1; k >= 0; --k) {
         const int j = k & 3;
         const bool outer = (j == 0) || (j == 3);
         if (j != 3) rev_thin_kick<M>(s, l, pa, pb, j == 1 ? K2 : K1, pm, g);
         if (EXACT) {
-            if (j != 3 || k == 4 * nsteps - 1) {
-                pz2 = c.A - s.px * s.px - s.py * s.py;
-                N = (outer ? L1 : L2) / sqrt(pz2);
-            }
+            if (j != 3 || k == 4 * nsteps - 1) N = (outer ? L1 : L2) / sqrt(c.A - s.px * s.px - s.py * s.py);
             s.x = s.x - N * s.px;
             s.y = s.y - N * s.py;
             s.z = s.z - N * c.bd + (outer ? L1b : L2b);
             const double gq = l.x * s.px + l.y * s.py + l.z * c.bd;
-            const double q = gq * N / pz2;
+            const double q = gq * (N * N * N) * (outer ? iL1sq : iL2sq);
             l.px = l.px + l.x * N + q * s.px;
             l.py = l.py + l.y * N + q * s.py;
             l.d = l.d + l.z * N - q * c.bd;
@@ -294,7 +295,7 @@ __device__ __forceinline__ void rev_bend_edge(P6& r, L6& l, double h, double c, 
     const double pzn = pxyz(D, pxn, r.py);
     const double num = r.x * (r.px * s2 + s * s * (2.0 * pz - h * r.x));
     const double den = pzn + pz * c - r.px * s;
-    const double dasin = asin_ool(jclamp(r.px / d2)) - asin_ool(jclamp(pxn / d2));
+    const double dasin = libm::asin(jclamp(r.px / d2)) - libm::asin(jclamp(pxn / d2));
     const double ih = 1.0 / h, ipz = 1.0 / pz, ipzn = 1.0 / pzn, id2 = 1.0 / d2, iden = 1.0 / den;
     const double lds = l.y * r.py * ih + l.z * dp1 * ih;  // cotangent of dasin
     const double lnum = l.x * iden;
@@ -503,7 +504,7 @@ __device__ __forceinline__ void rev_body_init(const P6& r, double h, double dp1,
     c.ih = 1.0 / h;
     c.pzo = pxyz(c.D, r.px, r.py);
     c.ipzo = 1.0 / c.pzo;
-    c.aso = asin_ool(jclamp(r.px * c.id2));
+    c.aso = libm::asin(jclamp(r.px * c.id2));
 }
 
 __device__ __forceinline__ void rev_body_step(P6& r, L6& l, RevBody& c, double h, double L, double Lbeti, double cs,
@@ -511,7 +512,7 @@ __device__ __forceinline__ void rev_body_step(P6& r, L6& l, RevBody& c, double h
     const double pxo = r.px;  // forward output px'
     const double pzmxo = c.pzo - (1.0 + r.x * h);
     const double px = pxo * cs - pzmxo * sn;
-    const double asi = asin_ool(jclamp(px * c.id2));
+    const double asi = libm::asin(jclamp(px * c.id2));
     const double dasin = L + (asi - c.aso) * c.ih;  // forward dasin
     const double pz = pxyz(c.D, px, r.py);
     const double ipz = 1.0 / pz;
