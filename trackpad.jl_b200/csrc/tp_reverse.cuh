@@ -295,7 +295,7 @@ __device__ __forceinline__ void rev_bend_edge(P6& r, L6& l, double h, double c, 
     const double pzn = pxyz(D, pxn, r.py);
     const double num = r.x * (r.px * s2 + s * s * (2.0 * pz - h * r.x));
     const double den = pzn + pz * c - r.px * s;
-    const double dasin = libm::asin(jclamp(r.px / d2)) - libm::asin(jclamp(pxn / d2));
+    const double dasin = asin_ool(jclamp(r.px / d2)) - asin_ool(jclamp(pxn / d2));
     const double ih = 1.0 / h, ipz = 1.0 / pz, ipzn = 1.0 / pzn, id2 = 1.0 / d2, iden = 1.0 / den;
     const double lds = l.y * r.py * ih + l.z * dp1 * ih;  // cotangent of dasin
     const double lnum = l.x * iden;
@@ -504,7 +504,7 @@ __device__ __forceinline__ void rev_body_init(const P6& r, double h, double dp1,
     c.ih = 1.0 / h;
     c.pzo = pxyz(c.D, r.px, r.py);
     c.ipzo = 1.0 / c.pzo;
-    c.aso = libm::asin(jclamp(r.px * c.id2));
+    c.aso = asin_ool(jclamp(r.px * c.id2));
 }
 
 __device__ __forceinline__ void rev_body_step(P6& r, L6& l, RevBody& c, double h, double L, double Lbeti, double cs,
@@ -512,7 +512,7 @@ __device__ __forceinline__ void rev_body_step(P6& r, L6& l, RevBody& c, double h
     const double pxo = r.px;  // forward output px'
     const double pzmxo = c.pzo - (1.0 + r.x * h);
     const double px = pxo * cs - pzmxo * sn;
-    const double asi = libm::asin(jclamp(px * c.id2));
+    const double asi = asin_ool(jclamp(px * c.id2));
     const double dasin = L + (asi - c.aso) * c.ih;  // forward dasin
     const double pz = pxyz(c.D, px, r.py);
     const double ipz = 1.0 / pz;
