@@ -70,6 +70,8 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-adjoint", action="store_true", help="default workload: skip the adjoint ratio")
+    p.add_argument("--no-full-length", action="store_true",
+                   help="default workload: skip the one 1000-turn track of the whole beam")
     p.add_argument("--no-batched", action="store_true",
                    help="default workload: skip the batched forward and batched adjoint summaries")
     return p.parse_args()
@@ -279,6 +281,26 @@ def adjoint_ratio(tp, local, turns=256, n=65536, warmup=4, steps=1):
 # ---------------------------------------------------------------------------
 # Single-lattice tracking (default)
 # ---------------------------------------------------------------------------
+def full_length_track(tp, torch, w, init, coords, lost, lost_turn, lost_elem, st_last, local, sptr, peak,
+                      turns=1000):
+    """The DBA configuration at its own length: one ringpass! of the whole beam over 1000 turns, device
+    resident, with the launch configuration the tuner settled on for the 10-turn steps (no new trials)."""
+    coords.copy_(init)
+    lost.zero_()
+    torch.cuda.synchronize()
+    tp.ringpass_(coords.T, w["lat"], w["beam"], lost, turns, aperture=w["aperture"], lost_turn=lost_turn,
+                 lost_elem=lost_elem, schedule=st_last["schedule"], min_blocks=st_last["min_blocks"], stream=sptr)
+    st = tp.last_stats(local)
+    achieved = st["flops"] / (st["kernel_ms"] * 1e-3) / 1e12
+    return {"metric": "particle*element*turns/s FP64 (1000 turns)", "value": st["units"] / (st["kernel_ms"] * 1e-3),
+            "unit": "particle*element*turns/s", "turns": turns, "kernel_ms": st["kernel_ms"],
+            "survivors": st["survivors"], "particles": st["particles"],
+            "maps_evaluated_per_s": st["element_passes"] / (st["kernel_ms"] * 1e-3),
+            "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak},
+            "schedule": st["schedule"], "min_blocks": st["min_blocks"]}
+
+
 def main_track(args, tp, torch, rank, world, local, dist):
     w = workload(args, rank)
     lat, beam, aperture, turns = w["lat"], w["beam"], w["aperture"], w["turns"]
@@ -314,11 +336,13 @@ def main_track(args, tp, torch, rank, world, local, dist):
     e1 = torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize()
     e0.record(stream)
+    passes = 0.0
     for _ in range(args.steps):
         st = step()
         kernel_ms.append(st["kernel_ms"])
         flops += st["flops"]
         units += st["units"]
+        passes += st["element_passes"]
         launches += st["launches"]
     e1.record(stream)
     torch.cuda.synchronize()
@@ -370,6 +394,9 @@ def main_track(args, tp, torch, rank, world, local, dist):
     adj = bat = bat_adj = None
     if args.workload == "dba" and world == 1 and not args.no_adjoint:
         adj = adjoint_ratio(tp, local)
+    full = None
+    if args.workload == "dba" and world == 1 and not args.no_full_length:
+        full = full_length_track(tp, torch, w, init, coords, lost, lost_turn, lost_elem, st, local, sptr, peak)
     if args.workload == "dba" and world == 1 and not args.no_batched:
         # the batched forward (256 variants, 100-turn steps) and the batched
         # time-dependent adjoint ratio, under the same clock as the headline
@@ -394,9 +421,13 @@ def main_track(args, tp, torch, rank, world, local, dist):
                          "peak_source": "measured FP64 FMA throughput of this device (tp_probe_fp64_peak)",
                          "flops_per_launch": flops / args.steps, "kernel_ms": k_ms},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
+            # the maps actually evaluated (a lost particle's remaining turns are in the unit, not here)
+            "maps_evaluated_per_s": passes / elapsed if world == 1 else None,
         }
         if adj is not None:
             line["adjoint"] = adj
+        if full is not None:
+            line["full_length"] = full
         if bat is not None:
             line["batched"] = bat
         if bat_adj is not None:

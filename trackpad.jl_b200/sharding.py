@@ -98,7 +98,19 @@ def distributed_ringpass_adjoint(coords0, lat, beam, lost0, nturns, params, *, s
                                            lost_weight=lost_weight, **kw)
     st = tracking.last_stats()
     terms = local_terms(loss, grad, st["survivors"], st["particles"], lost_weight)
-    return combine_adjoint(terms, torch_all_reduce(group, device), lost_weight)
+    return combine_adjoint(terms, torch_all_reduce(group, _collective_device(group, device)), lost_weight)
+
+
+def _collective_device(group, device):
+    """Where a collective's tensors live: the given device, else the current
+    GPU for NCCL (which takes CUDA tensors only), else the host (gloo)."""
+    import torch.distributed as dist
+    if device is not None:
+        return device
+    if dist.get_backend(group) == "nccl":
+        import torch
+        return torch.device("cuda", torch.cuda.current_device())
+    return None
 
 
 def torch_all_gather(group=None, device=None):
@@ -175,7 +187,7 @@ def distributed_ringpass_(coords, lat, beam, lost_flags, nturns, *, group=None, 
 
     from . import tracking
     rank, world = dist.get_rank(group), dist.get_world_size(group)
-    coll_dev = device if dist.get_backend(group) == "nccl" else None
+    coll_dev = _collective_device(group, device)
 
     def track(c, lf, lt, le):
         if c.shape[0]:
