@@ -156,3 +156,22 @@ def test_core_kinds_fit_the_small_pool():
         st = tp.tpsa.last_stats()
         assert st["slots"] == 18 and st["slots_used"] <= 18
         _assert_same(np.stack([m.coef for m in dev]), _oracle_maps(lat, refs, order, nturns=2))
+
+
+def test_later_calls_size_the_pool_by_the_slots_used():
+    """The first call on a lattice program and order runs the full 18-series
+    pool and records the slots it used; later calls size the pool to that
+    (more maps resident per SM) and give the same bits."""
+    lat = W.fodo_ring()
+    beam = tp.Beam(E0)
+    refs = _refs(40, 23)
+    outs, seen = [], []
+    for _ in range(2):
+        dev = tp.tpsa.ringpass(lat, [tp.polyseries_variables(r, 5) for r in refs], beam, 1)
+        st = tp.tpsa.last_stats()
+        seen.append((st["slots"], st["slots_used"]))
+        outs.append(np.stack([m.coef for m in dev]))
+    assert seen[0][0] == 18 and 6 < seen[0][1] < 18
+    assert seen[1][0] == max(7, seen[0][1])
+    assert np.array_equal(outs[0], outs[1])
+    _assert_same(outs[1][:8], _oracle_maps(lat, refs[:8], 5, nturns=1))

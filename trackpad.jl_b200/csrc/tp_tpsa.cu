@@ -996,6 +996,10 @@ int fail(int st, const std::string& m) {
 }
 
 thread_local tp_tpsa_stats g_tpsa_stats{};
+// Slots the last call on a (lattice program, order) used; keyed by the
+// lattice's stamp (unique per program) and the order.
+std::mutex g_slot_mu;
+std::unordered_map<uint64_t, int> g_slot_cache;
 
 bool tpsa_kind_ok(int kind) {
     return kind != DK_EXACT_SBEND && kind != DK_LBEND && kind != DK_WIGGLER && kind >= 0 && kind < DK_COUNT;
@@ -1160,85 +1164,118 @@ TP_API int tp_tpsa_ringpass(tp_ctx* ctx, const tp_lattice* lat, double* maps, in
         rare = rare || (h.kind > DK_RF && h.kind != DK_LONG_RF_MAP && h.kind != DK_LORENTZ &&
                         h.kind != DK_INV_LORENTZ && h.kind != DK_RLC_WAKE && h.kind != DK_TAB_WAKE && h.kind != DK_NAN);
     }
-    const int slots = rare ? kSlotsRare : kSlotsCore;
-    const size_t pool_bytes = size_t(slots) * M * 8;
-    // shared memory when it leaves room for at least two maps per SM (one map
-    // per SM is latency-bound: order 6 ran 2.2x faster from an L2-resident
-    // global pool at three maps per SM than from shared memory at one)
-    bool in_smem = pool_bytes + 1024 <= ch.smem_optin;
-    int per_sm = 1;
-    if (in_smem) {
-        if (pool_bytes > 48 * 1024)
-            TPSA_CUDA(cudaFuncSetAttribute(tpsa_track, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pool_bytes)));
-        TPSA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tpsa_track, block, pool_bytes));
-        in_smem = per_sm >= 2;
+    const int slots_full = rare ? kSlotsRare : kSlotsCore;
+    // The pool's slot count bounds the maps resident per SM.  A lattice's
+    // series bodies take the same slots whatever the coefficients (allocation
+    // follows the code path, which follows the element kinds), so a call
+    // sizes the pool by what the previous call on this lattice program and
+    // order used; if that runs out (TE_SLOTS), it runs again with the full pool.
+    LatticeView lv;
+    lattice_view(lat, &lv);
+    const uint64_t slot_key = lv.stamp * 16 + uint64_t(order);
+    int slots = slots_full;
+    {
+        std::lock_guard<std::mutex> g(g_slot_mu);
+        auto it = g_slot_cache.find(slot_key);
+        if (it != g_slot_cache.end()) slots = std::max(7, std::min(slots_full, it->second));
     }
-    if (!in_smem) per_sm = 3;
-    const int64_t grid = std::min<int64_t>(nmaps, int64_t(ch.sm_count) * per_sm);
-    double* gpool = nullptr;
-    if (!in_smem) {
-        void* p = nullptr;
-        if ((st = ctx_scratch(ctx, kTpsaScratchPool, size_t(grid) * pool_bytes, &p)) != TP_OK) return st;
-        gpool = static_cast<double*>(p);
-    }
-    TArgs a{};
-    a.table = dtable;
-    a.nelem = L.nelem;
-    a.N = order;
-    a.M = M;
-    a.sched = L.sched_words ? dsched : nullptr;
-    a.sched_stride = L.sched_stride;
-    a.sched_turn0 = L.sched_turn0;
-    a.sched_nturns = L.sched_nturns;
-    a.mis = md.empty() ? nullptr : dmis;
-    a.otab = dotab;
-    a.pairs = dpairs;
-    a.olen = olen;
-    a.maps = static_cast<double*>(d_maps);
-    a.nmaps = nmaps;
-    a.gpool = gpool;
-    a.beti = beti;
-    a.nturns = nturns;
-    a.turn0 = turn0;
-    a.err = derr;
-    a.ops = dops;
-    a.slots = slots;
-    cudaEvent_t e0, e1;
-    TPSA_CUDA(cudaEventCreate(&e0));
-    TPSA_CUDA(cudaEventCreate(&e1));
-    cudaEventRecord(e0, s);
-    tpsa_track<<<int(grid), block, in_smem ? pool_bytes : 0, s>>>(a);
-    cudaEventRecord(e1, s);
-    cudaError_t le = cudaGetLastError();
-    int32_t herr = 0;
-    unsigned long long hops[3] = {0, 0, 0};
-    if (le == cudaSuccess) le = cudaMemcpyAsync(maps, d_maps, map_bytes, cudaMemcpyDeviceToHost, s);
-    if (le == cudaSuccess) le = cudaMemcpyAsync(&herr, derr, 4, cudaMemcpyDeviceToHost, s);
-    if (le == cudaSuccess) le = cudaMemcpyAsync(hops, dops, 24, cudaMemcpyDeviceToHost, s);
-    if (le == cudaSuccess) le = cudaStreamSynchronize(s);
-    float ms = 0.f;
-    if (le == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (le != cudaSuccess) return fail(TP_ECUDA, std::string("TPSA kernel: ") + cudaGetErrorString(le));
     tp_tpsa_stats& g = g_tpsa_stats;
-    g = tp_tpsa_stats{};
-    g.maps = nmaps;
-    g.order = order;
-    g.coefficients = M;
-    g.pairs = int64_t(T.pairs.size());
-    g.series_mul = double(hops[0]);
-    g.series_lin = double(hops[1]);
-    g.flops = g.series_mul * (2.0 * double(T.pairs.size()) - double(M)) + g.series_lin * double(M);
-    g.kernel_ms = ms;
-    g.grid = int32_t(grid);
-    g.block = block;
-    g.shared_pool = in_smem ? 1 : 0;
-    g.slots_used = int32_t(hops[2]);
-    g.slots = slots;
-    if (herr & TE_SLOTS) return fail(TP_ERANGE, "TPSA work slots exhausted (internal limit)");
-    if (herr & TE_KIND) return fail(TP_EUNSUPPORTED, "a record without a TPSA pass! method");
-    if (herr & TE_SCHED) return fail(TP_ERANGE, "turn outside the lattice schedule");
+    for (int attempt = 0;; ++attempt) {
+        const size_t pool_bytes = size_t(slots) * M * 8;
+        // shared memory when it leaves room for at least two maps per SM (one map
+        // per SM is latency-bound: order 6 ran 2.2x faster from an L2-resident
+        // global pool at three maps per SM than from shared memory at one)
+        bool in_smem = pool_bytes + 1024 <= ch.smem_optin;
+        int per_sm = 1;
+        if (in_smem) {
+            if (pool_bytes > 48 * 1024)
+                TPSA_CUDA(cudaFuncSetAttribute(tpsa_track, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               int(pool_bytes)));
+            TPSA_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, tpsa_track, block, pool_bytes));
+            in_smem = per_sm >= 2;
+        }
+        if (!in_smem) per_sm = 3;
+        const int64_t grid = std::min<int64_t>(nmaps, int64_t(ch.sm_count) * per_sm);
+        double* gpool = nullptr;
+        if (!in_smem) {
+            void* p = nullptr;
+            if ((st = ctx_scratch(ctx, kTpsaScratchPool, size_t(grid) * pool_bytes, &p)) != TP_OK) return st;
+            gpool = static_cast<double*>(p);
+        }
+        if (attempt > 0) {  // the first attempt overwrote the device maps: stage them again
+            TPSA_CUDA(cudaMemcpyAsync(d_maps, maps, map_bytes, cudaMemcpyHostToDevice, s));
+            TPSA_CUDA(cudaMemsetAsync(derr, 0, 48, s));
+        }
+        TArgs a{};
+        a.table = dtable;
+        a.nelem = L.nelem;
+        a.N = order;
+        a.M = M;
+        a.sched = L.sched_words ? dsched : nullptr;
+        a.sched_stride = L.sched_stride;
+        a.sched_turn0 = L.sched_turn0;
+        a.sched_nturns = L.sched_nturns;
+        a.mis = md.empty() ? nullptr : dmis;
+        a.otab = dotab;
+        a.pairs = dpairs;
+        a.olen = olen;
+        a.maps = static_cast<double*>(d_maps);
+        a.nmaps = nmaps;
+        a.gpool = gpool;
+        a.beti = beti;
+        a.nturns = nturns;
+        a.turn0 = turn0;
+        a.err = derr;
+        a.ops = dops;
+        a.slots = slots;
+        cudaEvent_t e0, e1;
+        TPSA_CUDA(cudaEventCreate(&e0));
+        TPSA_CUDA(cudaEventCreate(&e1));
+        cudaEventRecord(e0, s);
+        tpsa_track<<<int(grid), block, in_smem ? pool_bytes : 0, s>>>(a);
+        cudaEventRecord(e1, s);
+        cudaError_t le = cudaGetLastError();
+        int32_t herr = 0;
+        unsigned long long hops[3] = {0, 0, 0};
+        if (le == cudaSuccess) le = cudaMemcpyAsync(&herr, derr, 4, cudaMemcpyDeviceToHost, s);
+        if (le == cudaSuccess) le = cudaMemcpyAsync(hops, dops, 24, cudaMemcpyDeviceToHost, s);
+        if (le == cudaSuccess) le = cudaStreamSynchronize(s);
+        float ms = 0.f;
+        if (le == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        if (le != cudaSuccess) return fail(TP_ECUDA, std::string("TPSA kernel: ") + cudaGetErrorString(le));
+        if ((herr & TE_SLOTS) && slots < slots_full) {
+            std::lock_guard<std::mutex> lk(g_slot_mu);
+            g_slot_cache.erase(slot_key);
+            slots = slots_full;
+            continue;
+        }
+        g = tp_tpsa_stats{};
+        g.maps = nmaps;
+        g.order = order;
+        g.coefficients = M;
+        g.pairs = int64_t(T.pairs.size());
+        g.series_mul = double(hops[0]);
+        g.series_lin = double(hops[1]);
+        g.flops = g.series_mul * (2.0 * double(T.pairs.size()) - double(M)) + g.series_lin * double(M);
+        g.kernel_ms = ms;
+        g.grid = int32_t(grid);
+        g.block = block;
+        g.shared_pool = in_smem ? 1 : 0;
+        g.slots_used = int32_t(hops[2]);
+        g.slots = slots;
+        if (herr & TE_SLOTS) return fail(TP_ERANGE, "TPSA work slots exhausted (internal limit)");
+        if (herr & TE_KIND) return fail(TP_EUNSUPPORTED, "a record without a TPSA pass! method");
+        if (herr & TE_SCHED) return fail(TP_ERANGE, "turn outside the lattice schedule");
+        if (g.slots_used > 0) {
+            std::lock_guard<std::mutex> lk(g_slot_mu);
+            g_slot_cache[slot_key] = g.slots_used;
+        }
+        break;
+    }
+    TPSA_CUDA(cudaMemcpyAsync(maps, d_maps, map_bytes, cudaMemcpyDeviceToHost, s));
+    TPSA_CUDA(cudaStreamSynchronize(s));
     tp_stats* stt = ctx_stats(ctx);
     stt->h2d_bytes += map_bytes;
     stt->d2h_bytes += map_bytes;
