@@ -4,7 +4,7 @@ The package directory is `trackpad.jl_b200/`; load it under the module name
 `trackpad_b200` (see `load()` in the repository's entry scripts).  The public
 names mirror TrackPad.jl (`linepass!` -> `linepass_`, `ringpass!` -> `ringpass_`).
 """
-from . import _abi, optics, sharding, tpsa
+from . import _abi, checkpoint, optics, sharding, tpsa
 from .elements import (AbstractElement, AccelCavity, Corrector, CrabCavity, Drift, DriftSC, ERBend, ExactSBend,
                        HKicker, InvLorentzBoost, LongitudinalRFMap, LorentzBoost, M_ELECTRON, M_PROTON, Marker,
                        Octupole, OctupoleSC, Quadrupole, QuadrupoleSC, RBend, RBendSC, RFCavity, SBend, SBendSC,

@@ -36,6 +36,7 @@
 #include <cstring>
 #include <string>
 #include <mutex>
+#include <unordered_map>
 #include <vector>
 
 #include "tp_internal.h"
@@ -603,7 +604,15 @@ struct KTune {
     float best_ms = 0.f;
 };
 std::mutex g_ktune_mu;
-KTune g_ktune[16];
+// Per device, the tuning state of each configuration seen (a few dozen at most
+// in practice; the table is cleared when it grows past 256 entries).
+std::unordered_map<uint64_t, KTune> g_ktune[16];
+
+KTune& ktune_of(int device, uint64_t key) {
+    auto& m = g_ktune[device & 15];
+    if (m.size() > 256 && m.find(key) == m.end()) m.clear();
+    return m[key];
+}
 
 uint64_t ktune_key(std::initializer_list<int64_t> parts) {
     uint64_t h = 1469598103934665603ull;
@@ -618,7 +627,7 @@ uint64_t ktune_key(std::initializer_list<int64_t> parts) {
 // K for this call and whether it is a timing trial (*state: 1 trial, 2 settled).
 int32_t ktune_pick(int device, uint64_t key, int64_t ntot, int32_t nturns, int* state) {
     std::lock_guard<std::mutex> g(g_ktune_mu);
-    KTune& t = g_ktune[device & 15];
+    KTune& t = ktune_of(device, key);
     if (t.key != key) {
         t = KTune{};
         t.key = key;
@@ -638,7 +647,7 @@ int32_t ktune_pick(int device, uint64_t key, int64_t ntot, int32_t nturns, int* 
 
 void ktune_record(int device, uint64_t key, int32_t K, float ms, double rec) {
     std::lock_guard<std::mutex> g(g_ktune_mu);
-    KTune& t = g_ktune[device & 15];
+    KTune& t = ktune_of(device, key);
     if (t.key != key || t.ntried >= t.ncand || t.cand[t.ntried] != K) return;
     t.ms[t.ntried] = ms;
     t.rec[t.ntried] = rec;
@@ -654,7 +663,7 @@ void ktune_record(int device, uint64_t key, int32_t K, float ms, double rec) {
 
 float ktune_best_ms(int device, uint64_t key) {
     std::lock_guard<std::mutex> g(g_ktune_mu);
-    const KTune& t = g_ktune[device & 15];
+    const KTune& t = ktune_of(device, key);
     return t.key == key ? t.best_ms : 0.f;
 }
 
