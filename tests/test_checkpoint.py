@@ -40,10 +40,27 @@ def test_checkpoint_is_tied_to_its_lattice(tmp_path):
         tp.checkpoint.load(p)
 
 
+def _mixed_beam(lat, beam):
+    """Particles lost before, at and after turn 10 of 25, and survivors: the
+    oracle picks them from a wide DA grid and a wide Gaussian beam."""
+    import oracle_ref
+    cand = np.asfortranarray(np.concatenate([W.da_grid(30, 30, half=0.02),
+                                             W.gaussian(200, seed=61, sigma=(2e-3, 1e-4, 2e-3, 1e-4, 1e-2, 2e-3))]))
+    r = cand.copy(order="F")
+    rl = np.zeros(len(r), np.int64)
+    rlt = np.full(len(r), -1, np.int32)
+    oracle_ref.ringpass(lat, r, rl, tp.beti(beam), 25, aperture=(0.02, 0.02), lost_turn=rlt)
+    late = np.flatnonzero((rl == 1) & (rlt >= 10))
+    early = np.flatnonzero((rl == 1) & (rlt < 10))[:100]
+    alive = np.flatnonzero(rl == 0)
+    return np.asfortranarray(cand[np.sort(np.concatenate([late, early, alive]))]), len(late)
+
+
 @pytest.mark.gpu
 def test_resumed_track_equals_one_track(tmp_path):
     lat, beam = W.dba_ring(cells=3), W.dba_beam()
-    c0 = np.asfortranarray(np.concatenate([W.gaussian(500, seed=61), W.da_grid(12, 12, half=0.019)]))
+    c0, nlate = _mixed_beam(lat, beam)
+    assert nlate >= 10
     n = len(c0)
     ref = c0.copy(order="F")
     rl = np.zeros(n, np.int64)
