@@ -239,7 +239,7 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # Adjoint / forward ratio on the gradient workload
 # ---------------------------------------------------------------------------
-def adjoint_ratio(tp, local, turns=256, n=65536, warmup=4, steps=1):
+def adjoint_ratio(tp, local, turns=256, n=65536, warmup=6, steps=1):
     """Loss and gradient with respect to the 120 quadrupole k1 and 80 sextupole
     k2 of the DBA ring, 65,536 Gaussian particles, `turns` turns, against
     ringpass! of the same beam; device times from the library's CUDA events."""
@@ -602,7 +602,7 @@ def main_adjoint(args, tp, torch, rank, world, local, dist):
     import trackpad_b200.workloads as W
     turns = args.turns or 256
     clocks = Clocks(local)
-    r = adjoint_ratio(tp, local, turns=turns, warmup=max(4, args.warmup), steps=args.steps)
+    r = adjoint_ratio(tp, local, turns=turns, warmup=max(6, args.warmup), steps=args.steps)
     clk = clocks.stop()
     # end to end through the public API with host arrays (inputs staged every call)
     lat, beam = W.dba_ring(), W.dba_beam()
@@ -667,9 +667,9 @@ def batched_adjoint_summary(args, tp, torch, local):
     variants, 16,384 particles each, 50-turn steps) as an object of the
     default line."""
     w = batched_workload(argparse.Namespace(nvar=0, turns=0), 0, time_dependent=True)
-    m = batched_adjoint_measure(w, tp, torch, local, steps=2, warmup=4)
+    m = batched_adjoint_measure(w, tp, torch, local, steps=2, warmup=7)
     return {"metric": "batched adjoint/forward time ratio", "value": m["a"] / m["f"], "unit": "x",
-            "higher_is_better": False, "steps": 2, "warmup": 4,
+            "higher_is_better": False, "steps": 2, "warmup": 7,
             "config": {"workload": w["name"], "turns_per_step": w["turns"], "parameters": m["params"]},
             "batched_forward_ms": m["f"], "batched_adjoint_ms": m["a"], "reverse_ms": m["rev"],
             "checkpoint_every": m["st"]["checkpoint_every"], "checkpoint_bytes": m["st"]["checkpoint_bytes"],
@@ -678,7 +678,7 @@ def batched_adjoint_summary(args, tp, torch, local):
 
 def main_batched_adjoint(args, tp, torch, rank, world, local, dist):
     w = batched_workload(args, rank, time_dependent=True)
-    m = batched_adjoint_measure(w, tp, torch, local, args.steps, max(4, args.warmup))
+    m = batched_adjoint_measure(w, tp, torch, local, args.steps, max(7, args.warmup))
     st = m["st"]
     if rank == 0:
         line = {"metric": "adjoint/forward time ratio", "value": m["a"] / m["f"], "unit": "x", "n_gpus": world,

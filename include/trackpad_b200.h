@@ -181,8 +181,8 @@ typedef struct tp_opts {
                                   the reference's operations in its order (exact
                                   bends amplify a changed rounding to ~1e-11)     */
     int32_t block_size;        /* threads per block; 0 = autotuned                */
-    int32_t min_blocks;        /* tracking kernel instance: registers sized for 7,
-                                  6 or 5 resident 128-thread blocks per SM (more
+    int32_t min_blocks;        /* tracking kernel instance: registers sized for 8,
+                                  7, 6 or 5 resident 128-thread blocks per SM (more
                                   blocks hide more latency, fewer spill less);
                                   0 = autotuned.  The build with FMA contraction
                                   and tables with kinds outside the integrator
@@ -192,7 +192,7 @@ typedef struct tp_opts {
                                   variant's particles).  Autotuning (schedule and
                                   min_blocks 0): the first multi-turn calls of a
                                   configuration run static and lane refill at 7
-                                  blocks, then 6 and 5 blocks with the faster
+                                  blocks, then 8, 6 and 5 blocks with the faster
                                   schedule, each timed on the call's own work;
                                   later calls keep the fastest.  Every choice
                                   gives identical results                         */

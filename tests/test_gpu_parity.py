@@ -321,12 +321,12 @@ def test_batched_schedules_with_losses_equal_lattice_by_lattice(schedule):
 
 def test_autotuned_launch_settles_and_keeps_results():
     """schedule = min_blocks = 0: the first multi-turn calls try static and
-    refill at 7 resident blocks per SM, then 6 and 5 blocks with the faster
+    refill at 7 resident blocks per SM, then 8, 6 and 5 blocks with the faster
     schedule; later calls keep the fastest; every call gives the same bits."""
     lat, beam = W.dba_ring(cells=2), W.dba_beam()
     c0 = np.asfortranarray(np.concatenate([W.gaussian(300, seed=70), W.da_grid(16, 16)]))
     seen, outs = [], []
-    for _ in range(7):
+    for _ in range(8):
         c = c0.copy(order="F")
         l = np.zeros(len(c), np.int64)
         tp.ringpass_(c, lat, beam, l, 6, aperture=0.02)
@@ -334,15 +334,15 @@ def test_autotuned_launch_settles_and_keeps_results():
         seen.append((st["schedule"], st["min_blocks"]))
         outs.append((c, l))
     assert seen[0] == (1, 7) and seen[1] == (2, 7)
-    assert [m for _, m in seen[2:4]] == [6, 5] and seen[2][0] == seen[3][0]
-    assert seen[4] == seen[5] == seen[6] and seen[4] in seen[:4]
+    assert [m for _, m in seen[2:5]] == [8, 6, 5] and seen[2][0] == seen[3][0] == seen[4][0]
+    assert seen[5] == seen[6] == seen[7] and seen[5] in seen[:5]
     for c, l in outs[1:]:
         assert np.array_equal(c, outs[0][0]) and np.array_equal(l, outs[0][1])
 
 
-@pytest.mark.parametrize("minb", [5, 6, 7])
+@pytest.mark.parametrize("minb", [5, 6, 7, 8])
 def test_every_occupancy_instance_gives_the_same_bits(minb):
-    """The kernel instances sized for 5, 6 and 7 resident blocks per SM, single
+    """The kernel instances sized for 5, 6, 7 and 8 resident blocks per SM, single
     lattice and batched, bit-identical to the oracle / to each other."""
     lat, beam = W.dba_ring(cells=3), W.dba_beam()
     c0 = np.asfortranarray(np.concatenate([W.gaussian(500, seed=71), W.da_grid(12, 12)]))

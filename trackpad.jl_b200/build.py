@@ -44,6 +44,7 @@ def build(verbose=False, ptxas_info=False):
     units = [
         ("tp_track_fast.o", "tp_track.cu", ["-DTP_NS=fast", "-fmad=true"]),
         ("tp_track_strict.o", "tp_track.cu", ["-DTP_NS=strict", "-fmad=false", "-DTP_OCC_VARIANTS"]),
+        ("tp_track_strict_low.o", "tp_track.cu", ["-DTP_NS=strict_low", "-fmad=false", "-DTP_OCC_LOW"]),
         ("tp_track_checked.o", "tp_track.cu", ["-DTP_NS=checked", "-fmad=false", "-DTP_BOUNDS_CHECK"]),
         ("tp_runtime.o", "tp_runtime.cu", ["-fmad=false"]),
         ("tp_adjoint.o", "tp_adjoint.cu", ["-fmad=false"]),

@@ -78,7 +78,7 @@ bool records_have_rare(const double* recs, size_t words);
 // Kernel launchers (tp_track.cu, compiled once with and once without FMA
 // contraction).  Return a cudaError_t value.  `minb` selects the kernel
 // instance whose registers are sized for that many resident 128-thread blocks
-// per SM (5, 6 or 7 in the build without contraction, 7 in the other; tables
+// per SM (5, 6, 7 or 8 in the build without contraction, 7 in the other; tables
 // with kinds outside the integrator core always run 7); minb_track_* maps a
 // request to the instance that runs.
 constexpr int kTrackMaxBlock = 128;  // launch bound of the tracking kernels
@@ -88,6 +88,12 @@ int occupancy_track_fast(int block, int minb, size_t smem, int* blocks_per_sm);
 int occupancy_track_strict(int block, int minb, size_t smem, int* blocks_per_sm);
 int minb_track_fast(int minb);
 int minb_track_strict(int minb);
+// The instances sized for 5 and 6 resident blocks of the build without
+// contraction (a second unit of that build; minb_track_strict_low returns 0 for
+// counts it does not hold).
+int launch_track_strict_low(const TrackArgs& a, int grid, int block, int minb, size_t smem, void* stream);
+int occupancy_track_strict_low(int block, int minb, size_t smem, int* blocks_per_sm);
+int minb_track_strict_low(int minb);
 // The bounds-checked build (no contraction, tp_opts.bounds_check).
 int launch_track_checked(const TrackArgs& a, int grid, int block, int minb, size_t smem, void* stream);
 int occupancy_track_checked(int block, int minb, size_t smem, int* blocks_per_sm);

@@ -48,11 +48,12 @@ constexpr int kMaxDevices = 16;
 
 // Online choice of the launch configuration: the particle scheduling (1 =
 // static, 2 = lane refill) and the kernel instance whose registers are sized
-// for 7, 6 or 5 resident blocks per SM.  Every configuration gives
+// for 7, 8, 6 or 5 resident blocks per SM.  Every configuration gives
 // bit-identical results, so the first calls of a configuration key (sizes,
 // turns, drift, build, lattice version) each run one candidate on the caller's
 // own work, timed with the call's CUDA events: first the two schedules at 7
-// resident blocks, then 6 and 5 with the faster schedule.  Later calls keep the
+// resident blocks, then 8, 6 and 5 with the faster schedule (batched pooled
+// refill: then folds 2 and 4).  Later calls keep the
 // fastest candidate.  What the caller fixes in tp_opts is not tuned.
 struct LaunchCand {
     int sched = 1, minb = 7;
@@ -61,8 +62,8 @@ struct LaunchCand {
 
 struct LaunchTune {
     uint64_t key = 0;
-    LaunchCand cand[6];
-    float ms[6] = {};
+    LaunchCand cand[8];
+    float ms[8] = {};
     int ncand = 0, ntried = 0;
     int stage = 0;       // 0: schedules, 1: resident blocks, 2: batched refill folds, 3: settled
     LaunchCand best;
@@ -106,11 +107,11 @@ LaunchCand tune_pick(LaunchTune& t, uint64_t key, int fixed_sched, int fixed_min
     while (t.ntried == t.ncand && t.stage < 3) {
         const LaunchCand b = t.cand[tune_argmin(t)];
         if (t.stage == 0 && !fixed_minb && nminb > 1) {
-            for (int k = 1; k < nminb && t.ncand < 6; ++k) t.cand[t.ncand++] = {b.sched, minbs[k], 1};
+            for (int k = 1; k < nminb && t.ncand < 8; ++k) t.cand[t.ncand++] = {b.sched, minbs[k], 1};
             t.stage = 1;
         } else if (t.stage <= 1 && folds && b.sched == 2) {
             for (int f : {2, 4})
-                if (t.ncand < 6) t.cand[t.ncand++] = {2, b.minb, f};
+                if (t.ncand < 8) t.cand[t.ncand++] = {2, b.minb, f};
             t.stage = 2;
         } else {
             t.best = b;
@@ -141,29 +142,38 @@ TrackBuild track_build(const tp_opts& o) {
     return o.fp_contract ? TB_FAST : TB_STRICT;
 }
 
+// The strict build's 5- and 6-block instances live in a second unit.
+bool strict_low(const TrackArgs* a, int minb) {
+    return minb_track_strict_low(minb) == minb && minb > 0 && (a == nullptr || !a->rare);
+}
+
 int track_launch(TrackBuild b, const TrackArgs& a, int grid, int block, int minb, size_t smem, void* stream) {
     if (b == TB_CHECKED) return launch_track_checked(a, grid, block, minb, smem, stream);
-    if (b == TB_STRICT) return launch_track_strict(a, grid, block, minb, smem, stream);
+    if (b == TB_STRICT)
+        return strict_low(&a, minb) ? launch_track_strict_low(a, grid, block, minb, smem, stream)
+                                    : launch_track_strict(a, grid, block, minb, smem, stream);
     return launch_track_fast(a, grid, block, minb, smem, stream);
 }
 
 int track_occupancy(TrackBuild b, int block, int minb, size_t smem, int* bps) {
     if (b == TB_CHECKED) return occupancy_track_checked(block, minb, smem, bps);
-    if (b == TB_STRICT) return occupancy_track_strict(block, minb, smem, bps);
+    if (b == TB_STRICT)
+        return strict_low(nullptr, minb) ? occupancy_track_strict_low(block, minb, smem, bps)
+                                         : occupancy_track_strict(block, minb, smem, bps);
     return occupancy_track_fast(block, minb, smem, bps);
 }
 
 int track_minb(TrackBuild b, int minb) {
     if (b == TB_CHECKED) return minb_track_checked(minb);
-    if (b == TB_STRICT) return minb_track_strict(minb);
+    if (b == TB_STRICT) return strict_low(nullptr, minb) ? minb : minb_track_strict(minb);
     return minb_track_fast(minb);
 }
 
 bool pick_launch(LaunchTune* tu, std::mutex* mu, uint64_t key, const tp_opts& o, int nturns, TrackBuild build,
                  bool rare, bool batched, LaunchCand* out) {
-    int minbs[3] = {7, 6, 5};
+    int minbs[4] = {7, 8, 6, 5};
     int nminb = 1;
-    if (!rare && track_minb(build, 5) == 5 && track_minb(build, 6) == 6) nminb = 3;
+    if (!rare && track_minb(build, 5) == 5 && track_minb(build, 6) == 6 && track_minb(build, 8) == 8) nminb = 4;
     const int fixed_minb = o.min_blocks > 0 ? track_minb(build, o.min_blocks) : 0;
     const int fixed_sched = o.schedule == 1 || o.schedule == 2 ? o.schedule : 0;
     const bool folds = batched && fixed_sched != 1;

@@ -45,14 +45,14 @@ using namespace tp::dev;
 #define TP_MAX_BLOCK 128
 #endif
 // Resident 128-thread blocks per SM the register allocation is sized for
-// (MINB, a template parameter of the kernels): 7 gives 72 registers and 28
-// warps per SM, 6 gives 80 registers, 5 gives 96.  Measured on the DBA step
-// with the element table read through L1 (where the spilled stack lives): 4
-// blocks 697 ms, 5 blocks 638 ms, 6 blocks 626 ms, 7 blocks 611 ms, 8 blocks
-// 630 ms.  Fewer registers spill more, more warps hide more latency; which
-// wins depends on the lattice and the schedule, so the build that runs the
-// reference's operation order (TP_OCC_VARIANTS) carries 5, 6 and 7 for the
-// integrator-core kernels and the host picks one by timing.
+// (MINB, a template parameter of the kernels): 8 gives 64 registers and 32
+// warps per SM, 7 gives 72 registers and 28 warps, 6 gives 80 registers, 5
+// gives 96.  Fewer registers spill more, more warps hide more latency; which
+// wins depends on the lattice, the schedule and the code (8 blocks beat 7 on
+// the DBA step by 1.5 % and lost by 4-7 % on the 256-variant batch), so the
+// build that runs the reference's operation order carries 5, 6, 7 and 8 for
+// the integrator-core kernels (in two units, see carried_minb) and the host
+// picks one by timing.
 constexpr int kMinBlocksDefault = 7;
 constexpr int kMaxBlock = TP_MAX_BLOCK;
 constexpr long long kTmaSpinLimit = 1ll << 22;  // bounded mbarrier wait
@@ -379,11 +379,16 @@ int launch_t(const TrackArgs& a, int grid, int block, size_t smem, cudaStream_t 
     return int(cudaGetLastError());
 }
 
-// Resident-block counts this build carries for the integrator-core kernels
-// (tables with rare kinds always use the default).
-int clamp_minb(int minb) {
-#ifdef TP_OCC_VARIANTS
-    return (minb == 5 || minb == 6) ? minb : kMinBlocksDefault;
+// Resident-block counts this translation unit carries.  The build without
+// contraction is split in two units that compile in parallel: TP_OCC_VARIANTS
+// carries the default 7 (every kind) and 8 (integrator core), TP_OCC_LOW
+// carries 5 and 6 (integrator core) and nothing else; the other builds carry
+// the default only.  carried_minb returns 0 for a count the unit does not hold.
+int carried_minb(int minb) {
+#if defined(TP_OCC_LOW)
+    return (minb == 5 || minb == 6) ? minb : 0;
+#elif defined(TP_OCC_VARIANTS)
+    return minb == 8 ? 8 : kMinBlocksDefault;
 #else
     (void)minb;
     return kMinBlocksDefault;
@@ -392,18 +397,24 @@ int clamp_minb(int minb) {
 
 template <bool EXACT, bool REFILL>
 int launch_r(const TrackArgs& a, int grid, int block, int minb, size_t smem, cudaStream_t st) {
-    if (a.rare) return launch_t<EXACT, REFILL, true, kMinBlocksDefault>(a, grid, block, smem, st);
-#ifdef TP_OCC_VARIANTS
+#if defined(TP_OCC_LOW)
+    if (a.rare) return int(cudaErrorInvalidValue);  // tables with rare kinds run the default instance
     if (minb == 5) return launch_t<EXACT, REFILL, false, 5>(a, grid, block, smem, st);
     if (minb == 6) return launch_t<EXACT, REFILL, false, 6>(a, grid, block, smem, st);
+    return int(cudaErrorInvalidValue);
+#else
+    if (a.rare) return launch_t<EXACT, REFILL, true, kMinBlocksDefault>(a, grid, block, smem, st);
+#if defined(TP_OCC_VARIANTS)
+    if (minb == 8) return launch_t<EXACT, REFILL, false, 8>(a, grid, block, smem, st);
 #endif
     (void)minb;
     return launch_t<EXACT, REFILL, false, kMinBlocksDefault>(a, grid, block, smem, st);
+#endif
 }
 
 int launch(const TrackArgs& a, int grid, int block, int minb, size_t smem, void* stream) {
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    minb = a.rare ? kMinBlocksDefault : clamp_minb(minb);
+    minb = carried_minb(minb);
     if (a.nvar > 0) smem = 0;
     if (a.exact && a.refill) return launch_r<true, true>(a, grid, block, minb, smem, st);
     if (a.exact) return launch_r<true, false>(a, grid, block, minb, smem, st);
@@ -423,15 +434,18 @@ int occupancy_t(int block, size_t smem, int* blocks_per_sm) {
 }
 
 int occupancy(int block, int minb, size_t smem, int* blocks_per_sm) {
-    minb = clamp_minb(minb);
-#ifdef TP_OCC_VARIANTS
+    minb = carried_minb(minb);
+#if defined(TP_OCC_LOW)
     if (minb == 5) return occupancy_t<5>(block, smem, blocks_per_sm);
     if (minb == 6) return occupancy_t<6>(block, smem, blocks_per_sm);
+    return int(cudaErrorInvalidValue);
+#else
+#if defined(TP_OCC_VARIANTS)
+    if (minb == 8) return occupancy_t<8>(block, smem, blocks_per_sm);
 #endif
     return occupancy_t<kMinBlocksDefault>(block, smem, blocks_per_sm);
+#endif
 }
-
-int carried_minb(int minb) { return clamp_minb(minb); }
 
 }  // namespace TP_NS
 

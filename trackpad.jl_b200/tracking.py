@@ -399,7 +399,7 @@ def ringpass_(coords, lat, beam, lost_flags, nturns, *, time=0.0, dt_turn=0.0, t
     linearised drift (USE_EXACT_HAMILTONIAN = false); `contract=True` runs the
     kernel built with FMA contraction (faster; its rounding differs from the
     reference's operation order); `schedule` (1 static, 2 lane refill) and
-    `min_blocks` (kernel instance sized for 7, 6 or 5 resident blocks per SM)
+    `min_blocks` (kernel instance sized for 8, 7, 6 or 5 resident blocks per SM)
     fix what the autotuner otherwise picks (0); `bounds_check=True` runs the
     kernels that check every element-table record and particle index before
     reading it (a violation raises with TP_EDEVICE).
