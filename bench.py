@@ -65,6 +65,9 @@ def parse():
     p.add_argument("--turns", type=int, default=0, help="turns per step (0: the workload's default)")
     p.add_argument("--nvar", type=int, default=0, help="variants of the batched workloads (0: default)")
     p.add_argument("--contract", action="store_true", help="kernels built with FMA contraction")
+    p.add_argument("--min-blocks", type=int, default=0,
+                   help="dba/fodo workloads: kernel instance sized for 8, 7, 6 or 5 resident blocks per SM "
+                        "(0: chosen by the launch tuner)")
     p.add_argument("--table-smem", action="store_true",
                    help="stage element tables into shared memory (default: read through the L1 cache)")
     p.add_argument("--no-e2e", action="store_true")
@@ -320,7 +323,7 @@ def main_track(args, tp, torch, rank, world, local, dist):
         coords.copy_(init)
         lost.zero_()
         tp.ringpass_(coords.T, lat, beam, lost, turns, aperture=aperture, lost_turn=lost_turn, lost_elem=lost_elem,
-                     contract=args.contract, stream=sptr)
+                     contract=args.contract, min_blocks=args.min_blocks, stream=sptr)
         st = tp.last_stats(local)
         flush.fill_(1)  # L2 flush between timed iterations
         return st
@@ -379,7 +382,7 @@ def main_track(args, tp, torch, rank, world, local, dist):
             hl[...] = 0
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            tp.ringpass_(hc_f, lat, beam, hl, turns, aperture=aperture)
+            tp.ringpass_(hc_f, lat, beam, hl, turns, aperture=aperture, min_blocks=args.min_blocks)
             t1 = time.perf_counter()
             stt = tp.last_stats(local)
             if i > 0:
