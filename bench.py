@@ -43,11 +43,18 @@ L2_FLUSH_BYTES = 256 << 20
 SIGMA_LOSS = 1e-4      # sigma_x of the beam-size loss
 LOST_WEIGHT = 1e3
 
-# DRAM bytes per particle of one tracking launch: ncu capture of track_single on
-# the DBA ring, 135,168 particles (one full wave) x 10 turns, 1.324 GB read +
-# written (dram__bytes.sum.per_second x gpu__time_duration), almost all of it
-# the write-back of spilled stack lines.  Scaled by the launch's particle count.
-DRAM_BYTES_PER_PARTICLE = 1.3236e9 / 135168
+# DRAM bytes per particle of one tracking launch, by the kernel instance's
+# resident blocks per SM: ncu captures of track_single on the DBA ring, 135,168
+# particles x 10 turns, dram__bytes.sum.per_second x gpu__time_duration (7
+# blocks, 72 registers: 1.324 GB; 8 blocks, 64 registers: 2.302 GB), almost all
+# of it the write-back of spilled stack lines.  Scaled by the launch's particle
+# count; instances without a capture report no traffic.
+DRAM_BYTES_PER_PARTICLE_BY_MINB = {7: 1.3236e9 / 135168, 8: 2.3021e9 / 135168}
+
+
+def dram_traffic(min_blocks, n):
+    per = DRAM_BYTES_PER_PARTICLE_BY_MINB.get(int(min_blocks))
+    return None if per is None else per * n
 
 
 def parse():
@@ -328,7 +335,10 @@ def main_track(args, tp, torch, rank, world, local, dist):
         flush.fill_(1)  # L2 flush between timed iterations
         return st
 
-    for _ in range(args.warmup):
+    # at least 5 warm-up steps: the launch tuner's trials (2 schedules at 7
+    # blocks, then 8, 6 and 5 blocks) run on the first five calls
+    n_warm = max(5, args.warmup)
+    for _ in range(n_warm):
         step()
     torch.cuda.synchronize()
     if dist:
@@ -413,14 +423,17 @@ def main_track(args, tp, torch, rank, world, local, dist):
             "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded Philox Gaussian beam + DA grid)",
             "config": {"workload": w["name"], "turns_per_step": turns, "particles_per_gpu": n,
-                       "elements": len(lat), "l2": "flushed between timed steps (256 MiB write)",
+                       "elements": len(lat), "warmup_steps_run": n_warm,
+                       "l2": "flushed between timed steps (256 MiB write)",
                        "fp": "FMA contraction" if args.contract else "no FMA contraction (reference operation order)",
                        "element_table": "shared memory (TMA bulk copy)" if args.table_smem else "L1 cache"},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": DRAM_BYTES_PER_PARTICLE * n,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch on "
-                                           "135,168 particles x 10 turns (one full wave), scaled by particles; "
-                                           "almost all of it is the write-back of spilled stack lines",
+                         "frac": achieved / peak, "traffic": dram_traffic(st["min_blocks"], n),
+                         "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch of the "
+                                           f"{st['min_blocks']}-block instance on 135,168 particles x 10 turns, "
+                                           f"scaled by particles; almost all of it is the write-back of spilled "
+                                           f"stack lines",
+                         "min_blocks": st["min_blocks"], "schedule": st["schedule"],
                          "peak_source": "measured FP64 FMA throughput of this device (tp_probe_fp64_peak)",
                          "flops_per_launch": flops / args.steps, "kernel_ms": k_ms},
             "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches, "clocks": clk,
@@ -536,8 +549,8 @@ def batched_summary(args, tp, torch, local):
 def main_batched(args, tp, torch, rank, world, local, dist):
     w = batched_workload(args, rank)
     n = w["coords"].shape[0]
-    # at least 7 warm-up steps: the launch tuner's trials (schedules, resident
-    # blocks, refill folds) run on the first six calls
+    # at least 7 warm-up steps: the launch tuner's trials (2 schedules at 7 blocks,
+    # then 8, 6 and 5 blocks, then 2 refill folds if refill won) run on the first seven calls
     m = batched_measure(w, tp, torch, local, args.steps, max(7, args.warmup), dist)
     t = torch.tensor([m["elapsed"], m["units"]], dtype=torch.float64, device=torch.device("cuda", local))
     if dist:
@@ -588,8 +601,9 @@ def main_batched(args, tp, torch, rank, world, local, dist):
                        "l2": "flushed between timed steps (256 MiB write)",
                        "fp": "no FMA contraction (reference operation order)"},
             "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                         "frac": achieved / peak, "traffic": DRAM_BYTES_PER_PARTICLE * n,
-                         "traffic_source": "per-particle DRAM bytes of the single-lattice capture, scaled",
+                         "frac": achieved / peak, "traffic": dram_traffic(st["min_blocks"], n),
+                         "traffic_source": "per-particle DRAM bytes of the single-lattice capture of the same "
+                                           "instance, scaled",
                          "peak_source": "measured FP64 FMA throughput of this device (tp_probe_fp64_peak)",
                          "flops_per_launch": m["flops"] / args.steps, "kernel_ms": m["kernel_ms"]},
             "lattice_by_lattice": lbl, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": m["launches"],

@@ -107,7 +107,7 @@ __device__ __forceinline__ void bend_kick(P6& s, const double* pa, const double*
 
 // symplectic4_pass (src/tracking.jl:317-341) for one multipole record.
 template <int M, bool EXACT>
-__device__ __noinline__ void multipole(P6& s, const double* w, int nsteps, double beti) {
+__device__ __forceinline__ void multipole_body(P6& s, const double* w, int nsteps, double beti) {
     const double L1 = w[mp::L1], L2 = w[mp::L2], K1 = w[mp::K1], K2 = w[mp::K2];
     double pa[M + 1], pb[M + 1];
 #pragma unroll
@@ -142,6 +142,16 @@ __device__ __noinline__ void multipole(P6& s, const double* w, int nsteps, doubl
         }
         if (j != 3) thin_kick<M>(s, pa, pb, j == 1 ? K2 : K1);
     }
+}
+
+// Out of line for the orders lattices use rarely (0: a body with no field, 3:
+// octupoles).  Quadrupoles (order 1) and sextupoles (order 2) run inline in the
+// element loop: a call there saves and restores the caller's live registers
+// through the stack at every magnet, and inlining the two made the DBA step
+// 6 % faster, the 256-variant batch 5 % and the gradient's forward sweep 9 %.
+template <int M, bool EXACT>
+__device__ __noinline__ void multipole(P6& s, const double* w, int nsteps, double beti) {
+    multipole_body<M, EXACT>(s, w, nsteps, beti);
 }
 
 // true when 0/opd is zero, i.e. `e - 0/(1+delta)` equals e exactly.
@@ -954,8 +964,8 @@ __device__ __forceinline__ bool apply_record(P6& s, const double* rec, const Rec
         case DK_MULTIPOLE:
             switch (h.order) {
                 case 0: multipole<0, EXACT>(s, w, h.nsteps, beti); break;
-                case 1: multipole<1, EXACT>(s, w, h.nsteps, beti); break;
-                case 2: multipole<2, EXACT>(s, w, h.nsteps, beti); break;
+                case 1: multipole_body<1, EXACT>(s, w, h.nsteps, beti); break;
+                case 2: multipole_body<2, EXACT>(s, w, h.nsteps, beti); break;
                 default: multipole<3, EXACT>(s, w, h.nsteps, beti); break;
             }
             break;

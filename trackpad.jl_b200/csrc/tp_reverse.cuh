@@ -142,8 +142,8 @@ __device__ __forceinline__ void rev_bend_kick(P6& s, L6& l, const double* pa, co
 // Multipole: symplectic4_pass (src/tracking.jl:317-341) run backwards.
 // ---------------------------------------------------------------------------
 template <int M, bool EXACT>
-__device__ __noinline__ void rev_multipole(P6& s, L6& l, const double* w, int nsteps, double beti, int pm,
-                                           double& g) {
+__device__ __forceinline__ void rev_multipole_body(P6& s, L6& l, const double* w, int nsteps, double beti, int pm,
+                                                   double& g) {
     const double L1 = w[mp::L1], L2 = w[mp::L2], K1 = w[mp::K1], K2 = w[mp::K2];
     double pa[M + 1], pb[M + 1];
 #pragma unroll
@@ -179,6 +179,17 @@ __device__ __noinline__ void rev_multipole(P6& s, L6& l, const double* w, int ns
             rev_drift<EXACT>(s, l, outer ? L1 : L2, outer ? L1b : L2b, c);
         }
     }
+}
+
+// Out of line for the orders lattices use rarely (0: a body with no field, 3:
+// octupoles).  Quadrupoles (order 1) and sextupoles (order 2) run inline in the
+// sweep's element loop: a call there saves and restores the caller's live
+// registers through the stack at every magnet, and inlining the two made the
+// reverse sweep of the DBA gradient 24-28 % faster.
+template <int M, bool EXACT>
+__device__ __noinline__ void rev_multipole(P6& s, L6& l, const double* w, int nsteps, double beti, int pm,
+                                           double& g) {
+    rev_multipole_body<M, EXACT>(s, l, w, nsteps, beti, pm, g);
 }
 
 // ---------------------------------------------------------------------------
@@ -662,8 +673,8 @@ __device__ __forceinline__ bool reverse_core(P6& s, L6& l, const double* rec, co
         case DK_MULTIPOLE:
             switch (h.order) {
                 case 0: rev_multipole<0, EXACT>(s, l, w, h.nsteps, beti, pm, g); break;
-                case 1: rev_multipole<1, EXACT>(s, l, w, h.nsteps, beti, pm, g); break;
-                case 2: rev_multipole<2, EXACT>(s, l, w, h.nsteps, beti, pm, g); break;
+                case 1: rev_multipole_body<1, EXACT>(s, l, w, h.nsteps, beti, pm, g); break;
+                case 2: rev_multipole_body<2, EXACT>(s, l, w, h.nsteps, beti, pm, g); break;
                 default: rev_multipole<3, EXACT>(s, l, w, h.nsteps, beti, pm, g); break;
             }
             break;
