@@ -45,11 +45,12 @@ LOST_WEIGHT = 1e3
 
 # DRAM bytes per particle of one tracking launch, by the kernel instance's
 # resident blocks per SM: ncu captures of track_single on the DBA ring, 135,168
-# particles x 10 turns, dram__bytes.sum.per_second x gpu__time_duration (7
-# blocks, 72 registers: 1.324 GB; 8 blocks, 64 registers: 2.302 GB), almost all
-# of it the write-back of spilled stack lines.  Scaled by the launch's particle
-# count; instances without a capture report no traffic.
-DRAM_BYTES_PER_PARTICLE_BY_MINB = {7: 1.3236e9 / 135168, 8: 2.3021e9 / 135168}
+# particles x 10 turns, dram__bytes.sum.per_second x gpu__time_duration (8
+# blocks, 64 registers: 2.420 GB; 7 blocks, 72 registers: 1.324 GB, captured
+# with the multipole integrator out of line), almost all of it the write-back of
+# spilled stack lines.  Scaled by the launch's particle count; instances without
+# a capture report no traffic.
+DRAM_BYTES_PER_PARTICLE_BY_MINB = {7: 1.3236e9 / 135168, 8: 2.4199e9 / 135168}
 
 
 def dram_traffic(min_blocks, n):
