@@ -298,7 +298,7 @@ __device__ __forceinline__ void rev_yrot(P6& r, L6& l, double c, double s, doubl
 __device__ __forceinline__ void rev_bend_edge(P6& r, L6& l, double h, double c, double s, double s2, double theta,
                                               double thh, double beti) {
     const double dp1 = beti + r.d;
-    bend_edge(r, h, c, -s, -s2, -theta, -thh, dp1);  // inverse
+    bend_edge_body(r, h, c, -s, -s2, -theta, -thh, dp1);  // inverse, inline
     const double D = dp1 * dp1;
     const double pz = pxyz(D, r.px, r.py);
     const double d2 = pxyz(D, 0.0, r.py);
